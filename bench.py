@@ -1,0 +1,398 @@
+"""Benchmark of Myers candidate verification on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload 1..5]
+                    [--path plain|batched] [--impl ours|reference]
+
+One step = one verification pass over the whole batch of the workload (all
+candidates of all reads, inputs resident in HBM). Default workload: 1M reads
+of 1,000 bases, 11 candidates each (11M candidates), over a 3.1 Gbase
+synthetic reference -- the full-shape plain Myers configuration. Prints one
+JSON line (rank 0).
+
+  value     candidates/s over the timed steps, kernels on HBM-resident inputs
+            (N GPUs: each rank verifies its own seeded batch; the sum of
+            candidates / the slowest rank's time)
+  e2e       the same metric through the drop-in C API (initMyers /
+            sendMyersBuffer / receiveMyersBuffer) from pinned host buffers:
+            H2D of PEQ, query info and candidates and D2H of the results are
+            inside the timed region
+  roofline  the Myers kernel against the measured integer-ALU peak (3-input
+            logic ops/s probed in this run): achieved = word-steps x 11 ops
+            per launch / launch time
+  cpu_baseline  the reference's own CPU Myers (compiled from its sources into
+            oracle/_ref) on the host cores, on a bounded sample
+
+--impl reference times the reference's own CPU implementation instead (the
+GPU path of the reference targets sm_20..sm_50 only).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "myers-gpu_b200"))
+
+DIST = 0.2
+OPS_PER_WORD_STEP = 11  # the fused recurrence: PEQ select + 10 logic/add/shift ops
+
+WORKLOAD_NAMES = {
+    1: "plain-100b: 16 Mbase ref, 100K reads x 100 b, 11 cand/read (1.1M candidates)",
+    2: "plain-1000b: 3.1 Gbase ref, 1M reads x 1000 b, 11 cand/read (11M candidates)",
+    3: "batched-mixed: 3.1 Gbase ref, 2M reads of 100..1000 b, 1+Poisson(10) cand/read",
+    4: "batched-long: 3.1 Gbase ref, 100K reads of 1000..10000 b, 1+Poisson(4) cand/read",
+    5: "serving-mix: 3.1 Gbase ref, reads of 100..1000 b, 1..64 cand/read",
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", type=int, default=2, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--path", default=None, choices=["plain", "batched"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's reads (tests)")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def make_inputs(mg, k, scale, seed_offset, num_reads=None):
+    s = mg.workload_spec(k, scale=scale)
+    s.seed += 7919 * seed_offset
+    if num_reads is not None:
+        s.num_reads = min(s.num_reads, num_reads)
+    ref_size = s.ref_size
+    ref_words = mg.make_reference(ref_size, 1000 + (s.seed if k == 1 else 0))
+    w = mg.make_workload(s, ref_words)
+    return s, ref_words, ref_size, w
+
+
+def cpu_baseline(mg, k, args, full_cands):
+    """Reference CPU Myers (oracle/_ref) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = host_threads()
+    kind = "reference" if orc.have_reference() else "port"
+
+    def run(w, ref_words, ref_size):
+        if kind == "reference":
+            res, sec = orc.reference_verify_aligned(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST,
+                                                    nthreads=threads)
+        else:
+            t = time.perf_counter()
+            orc.verify(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST, nthreads=threads)
+            sec = time.perf_counter() - t
+        return sec
+
+    # probe with a few reads, then size the sample to the time budget
+    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0, num_reads=max(1, 2000 // (10 if k in (2, 4) else 1)))
+    sec = max(run(w, ref_words, ref_size), 1e-4)
+    per_read = sec / len(w["qinfo"])
+    n_reads = int(max(len(w["qinfo"]), min(s.num_reads, args.cpu_seconds / per_read)))
+    s.num_reads = n_reads
+    w = mg.make_workload(s, ref_words)
+    sec = run(w, ref_words, ref_size)
+    cps = len(w["cands"]) / sec
+    cells, _ = mg.cells(w["qinfo"], w["cands"], DIST)
+    return {"value": cps, "unit": "candidates/s", "cores": threads, "kind": kind,
+            "gcups": float(cells.sum() / sec / 1e9),
+            "sample": f"first {n_reads} reads ({len(w['cands'])} candidates) of the same seeded workload, "
+                      f"{sec:.1f} s of CPU time, OpenMP over {threads} threads"}
+
+
+def run_reference(args):
+    import myersgpu as mg
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    k = args.workload
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = host_threads()
+    kind = "reference" if orc.have_reference() else "port"
+    per_step = max(1.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0, num_reads=max(1, 2000 // (10 if k in (2, 4) else 1)))
+
+    def run(w):
+        if kind == "reference":
+            return orc.reference_verify_aligned(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST,
+                                                nthreads=threads)[1]
+        t = time.perf_counter()
+        orc.verify(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST, nthreads=threads)
+        return time.perf_counter() - t
+
+    sec = max(run(w), 1e-4)
+    s.num_reads = int(max(len(w["qinfo"]), min(s.num_reads, per_step / (sec / len(w["qinfo"])))))
+    w = mg.make_workload(s, ref_words)
+    for _ in range(args.warmup):
+        run(w)
+    times = [run(w) for _ in range(args.steps)]
+    t = float(np.mean(times))
+    cps = len(w["cands"]) / t
+    cells, _ = mg.cells(w["qinfo"], w["cands"], DIST)
+    line = {"impl": "reference", "metric": "candidates/s", "value": cps, "unit": "candidates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded)", "gcups": float(cells.sum() / t / 1e9),
+            "config": {"workload": WORKLOAD_NAMES[k], "distance": DIST, "window": "aligned"},
+            "cpu_baseline": {"value": cps, "unit": "candidates/s", "cores": threads, "kind": kind,
+                             "sample": f"each step: first {s.num_reads} reads ({len(w['cands'])} candidates) "
+                                       f"of the workload, OpenMP over {threads} threads"},
+            "e2e": {"value": cps, "unit": "candidates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    import myersgpu as mg
+    world, rank, local, dist = dist_setup(args)
+    torch.cuda.set_device(local)
+    k = args.workload
+    path = {"plain": mg.PATH_PLAIN, "batched": mg.PATH_BATCHED}[args.path or ("batched" if k in (3, 4, 5) else "plain")]
+    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, rank)
+    n_cands = len(w["cands"])
+    lengths = w["qinfo"]["size"]
+    cells, word_steps = mg.cells(w["qinfo"], w["cands"], DIST)
+    ws_total = float(word_steps.sum())
+
+    ref = mg.Reference(ref_words, ref_size)
+    ctx = mg.Context(n_cands)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to("cuda")
+
+    d_peq, d_qi, d_c = dev(w["peq"]), dev(w["qinfo"]), dev(w["cands"])
+    d_res = torch.empty(n_cands * 8, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    lo, hi = int(lengths.min()), int(lengths.max())
+
+    def step():
+        ctx.verify(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(), n_cands,
+                   DIST, d_res.data_ptr(), path=path, stream=sp, min_size=lo, max_size=hi)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches_per_step = ctx.launches()
+
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for i in range(args.steps):
+        step()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist is not None:
+        dist.barrier()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    elapsed = sum(step_ms) / 1e3
+    if dist is not None:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        tot = torch.tensor([float(n_cands), float(cells.sum())], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tot)
+        all_cands, all_cells = float(tot[0].item()), float(tot[1].item())
+    else:
+        all_cands, all_cells = float(n_cands), float(cells.sum())
+    value = all_cands * args.steps / elapsed
+    gcups = all_cells * args.steps / elapsed / 1e9
+
+    # parity spot check of the timed output against the oracle (a sample)
+    res = d_res.cpu().numpy().view(mg.RES)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    idx = np.random.default_rng(rank).choice(n_cands, size=min(2000, n_cands), replace=False)
+    sub = w["cands"][idx]
+    expect = orc.verify(w["peq"], w["qinfo"], sub, ref_words, ref_size, DIST)
+    parity = bool(np.array_equal(res[idx], expect))
+
+    # roofline: the dominant kernel is the whole step on the plain single-launch path
+    peak = mg.probe_int_peak(4000)
+    kernel_s = float(np.mean(step_ms)) / 1e3
+    achieved = ws_total * OPS_PER_WORD_STEP / kernel_s
+    hbm_bytes = float(len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * (16 + 8)
+                      + (word_steps / np.ceil(w["qinfo"]["size"][w["cands"]["query"]] / 32) / 2).sum())
+    peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak = json.load(open(peaks_file)).get("hbm_gbs") if os.path.exists(peaks_file) else 6650.0
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"traffic_workload{k}.json")
+    if os.path.exists(prof):
+        t = json.load(open(prof))
+        traffic = t["dram_bytes_per_candidate"] * n_cands
+
+    # end to end through the drop-in API
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(mg, args, ref_words, ref_size, w, path)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(mg, k, args, n_cands)
+
+    ctx.close()
+    ref.close()
+    if rank == 0:
+        line = {
+            "metric": "candidates/s", "value": value, "unit": "candidates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+            "gcups": gcups,
+            "config": {"workload": WORKLOAD_NAMES[k], "candidates_per_gpu": n_cands, "distance": DIST,
+                       "window": "aligned", "path": "batched" if path == mg.PATH_BATCHED else "plain",
+                       "l2": "inputs larger than L2 (3.1 Gbase reference = 1.55 GB resident)" if k != 1
+                       else "16 Mbase reference fits L2; candidates/PEQ stream from HBM",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "3-input logic op probe (LOP3, 8 independent chains) in this run",
+                         "ops_per_word_step": OPS_PER_WORD_STEP,
+                         "hbm": {"achieved_gbs": hbm_bytes / kernel_s / 1e9, "peak_gbs": hbm_peak,
+                                 "frac": hbm_bytes / kernel_s / 1e9 / hbm_peak}},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps,
+            "parity_sample": {"candidates": int(len(idx)), "bit_exact": parity},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_e2e(mg, args, ref_words, ref_size, w, path):
+    n_cands = len(w["cands"])
+    with tempfile.TemporaryDirectory() as tmp:
+        fn = os.path.join(tmp, "bench.4bits.ref")
+        with open(fn, "wb") as f:
+            f.write(np.array([len(ref_words), ref_size], dtype=np.uint32).tobytes())
+            ref_words.tofile(f)
+        need = len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * 32
+        mg.lib.myersSetMemoryBudget(int(need * 1.3) + (64 << 20))
+        avg = int(w["qinfo"]["size"].mean())
+        cpq = max(1, n_cands // max(1, len(w["qinfo"])))
+        bufs = mg.Buffers(fn, num_buffers=1, avg_query_size=avg, cands_per_query=cpq)
+    try:
+        bufs.set_path(path)
+        ne, nq, nc = bufs.capacity(0)
+        if ne < len(w["peq"]) or nq < len(w["qinfo"]) or nc < n_cands:
+            return {"value": None, "unit": "candidates/s", "note": f"buffer capacity too small {(ne, nq, nc)}"}
+        v_peq, v_qi, v_c, v_res = bufs.views(0)
+        v_peq[: len(w["peq"])] = w["peq"]
+        v_qi[: len(w["qinfo"])] = w["qinfo"]
+        v_c[:n_cands] = w["cands"]
+        for _ in range(max(1, args.warmup)):
+            bufs.send(0, DIST, len(w["peq"]), len(w["qinfo"]), n_cands)
+            mg.check(bufs.receive(0), "receive")
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            bufs.send(0, DIST, len(w["peq"]), len(w["qinfo"]), n_cands)
+            mg.check(bufs.receive(0), "receive")
+        el = time.perf_counter() - t
+        h2d = len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * 16
+        return {"value": n_cands * args.steps / el, "unit": "candidates/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(n_cands * 8),
+                "api": "initMyers buffers: fill pinned host buffers (untimed), then sendMyersBuffer + "
+                       "receiveMyersBuffer per step (H2D, kernels, D2H timed)"}
+    finally:
+        bufs.close()
+        mg.lib.myersSetMemoryBudget(0)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

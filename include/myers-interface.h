@@ -1,0 +1,258 @@
+/*
+ * myers-interface.h - C ABI of the B200 Myers candidate-verification library
+ * (libmyers_b200.so).
+ *
+ * The first part is a drop-in for the reference's public header
+ * (src-api/myers-interface.h:1-46 in achacond/myers-gpu): same types with the
+ * same layouts, same buffer getters and the same four main calls, with the
+ * same fatal error convention (print, then exit(EXIT_FAILURE)).
+ *
+ * The second part adds what the reference lacks: status-returning variants
+ * of the main calls, options (window mode, kernel path, memory budget), a
+ * stream-ordered entry point on device-resident inputs, and a serving loop.
+ *
+ * All entry points take plain pointers and sizes; there are no C++ or torch
+ * types in any signature.
+ */
+#ifndef MYERS_INTERFACE_H
+#define MYERS_INTERFACE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NUM_BITS         4
+#define NUM_BASES        5
+#define NUM_BASES_ENTRY  128
+#define SIZE_GPU_HW_WORD 32
+#define NUM_SUB_ENTRIES  (NUM_BASES_ENTRY / SIZE_GPU_HW_WORD)
+
+/* PEQ entry: 128 query bases. Bit i of bitmap[c][w] is set iff query base
+ * 32*w+i of this entry has code c (A0 C1 G2 T3 N4). Replaces the reference's
+ * qryEntry_t, src-api/myers-interface.h:10-12 (80 bytes). */
+typedef struct {
+    uint32_t bitmap[NUM_BASES][NUM_SUB_ENTRIES];
+} qryEntry_t;
+
+/* Result of one candidate: end column of the first minimum and its edit
+ * distance. Replaces resEntry_t, src-api/myers-interface.h:14-17. */
+typedef struct {
+    uint32_t column;
+    uint32_t score;
+} resEntry_t;
+
+/* Candidate: query index and reference base position (16 bytes with the
+ * compiler's padding). Replaces candInfo_t, src-api/myers-interface.h:19-22. */
+typedef struct {
+    uint32_t query;
+    uint64_t position;
+} candInfo_t;
+
+/* Query: first PEQ entry and length in bases. Replaces qryInfo_t,
+ * src-api/myers-interface.h:24-27. */
+typedef struct {
+    uint32_t posEntry;
+    uint32_t size;
+} qryInfo_t;
+
+/* ---------------------------------------------------------------------------
+ * Drop-in API (reference: src-api/myers-interface.h:30-46, src-api/myersGPU.c)
+ * ------------------------------------------------------------------------- */
+
+/* Library-owned pinned host buffers of one Myers buffer; the caller fills
+ * them in place between calls. Replaces the getters at
+ * src-api/myers-interface.h:31-34 (src-api/myersGPU.c:70-88). The reference
+ * declares them `inline`; here they are ordinary exported functions so that
+ * both C89-inline and C99 callers link. */
+qryEntry_t *getPEQBuffer(void *myersBuffer);
+candInfo_t *getCandidatesBuffer(void *myersBuffer);
+qryInfo_t  *getPEQInfoBuffer(void *myersBuffer);
+resEntry_t *getResultsBuffer(void *myersBuffer);
+
+/* Capacities of one buffer. Replace src-api/myers-interface.h:37-39
+ * (src-api/myersGPU.c:55-68). */
+uint32_t getMaxPEQEntries(void *myersBuffer);
+uint32_t getMaxCandidates(void *myersBuffer);
+uint32_t getMaxQueries(void *myersBuffer);
+
+/* Load the packed reference (`u32 numEntries, u32 size, u32 words[]`) once
+ * into device memory and create `numBuffers` buffers, each with its own
+ * stream on the current device, sized from the memory budget (see
+ * myersSetMemoryBudget). Returns 0. Replaces src-api/myers-interface.h:42
+ * (defined at src-api/myersGPU.c:284-344). */
+int initMyers(void ***myersBuffer, uint32_t numBuffers, const char *referenceFileName,
+              int32_t averageQuerySize, int32_t candidatesPerQuery);
+
+/* Enqueue the verification of the buffer's first numCandidates candidates on
+ * the buffer's stream and return; the buffer must not be touched until
+ * receiveMyersBuffer. `distance` is the error fraction: the window of a
+ * query of m bases spans (uint32_t)(m*(1+2*distance)) bases. Replaces
+ * src-api/myers-interface.h:44 (src-api/myersGPU.c:466-494). */
+void sendMyersBuffer(void *myersBuffer, float distance, uint32_t numPEQEntries,
+                     uint32_t numQueries, uint32_t numCandidates);
+
+/* Wait for the buffer; afterwards getResultsBuffer()[i] holds candidate i's
+ * result in caller order. Replaces src-api/myers-interface.h:45
+ * (src-api/myersGPU.c:515-524). */
+void receiveMyersBuffer(void *myersBuffer);
+
+/* Release every buffer, the streams and the device reference. Replaces
+ * src-api/myers-interface.h:46 (src-api/myersGPU.c:651-676). */
+void endMyers(void ***myersBuffer);
+
+/* ---------------------------------------------------------------------------
+ * Extensions (no counterpart in the reference unless stated)
+ * ------------------------------------------------------------------------- */
+
+/* Error codes. The first six keep the values of the reference's
+ * myersError_t (src-api/myers-common.h:13-24). */
+typedef enum {
+    MYERS_SUCCESS = 0,
+    MYERS_E_OPENING_FILE = 1,
+    MYERS_E_READING_FILE = 2,
+    MYERS_E_INSUFFICIENT_MEM_GPU = 3,
+    MYERS_E_ALLOCATE_MEM = 4,
+    MYERS_E_INCOMPATIBLE_GPU = 5,
+    MYERS_E_INVALID_ARGUMENT = 6,
+    MYERS_E_CAPACITY = 7,        /* more entries/queries/candidates than the buffer holds */
+    MYERS_E_QUERY_TOO_LONG = 8,  /* a query longer than MYERS_MAX_QUERY_BASES */
+    MYERS_E_CUDA = 9,            /* a CUDA runtime call failed */
+    MYERS_E_TIMEOUT = 10,        /* a bounded device-side wait gave up */
+    MYERS_E_NOT_READY = 11,      /* serving: request not finished yet */
+    MYERS_E_BUSY = 12            /* serving: admission refused (queue or budget full) */
+} myersStatus_t;
+
+/* Longest query (bases) the kernels verify: 32 lanes x 32 words x 32 bits. */
+#define MYERS_MAX_QUERY_BASES 32768u
+/* Longest window (columns) a result column can address. */
+#define MYERS_MAX_WINDOW_COLUMNS 65535u
+
+const char *myersGetErrorString(int status);
+
+/* Window semantics.
+ *  ALIGNED (default, the API's): the text starts at the packed word holding
+ *    the candidate position and spans 8*E columns, E = W/8 + (W%8 ? 2 : 1);
+ *    columns are counted from that word (src-api/coreMyersGPU-CC50.cu:131-166).
+ *  EXACT: the text starts at the position and spans W columns; columns are
+ *    counted from the position (src/myers-4bits.c:75-153). */
+enum { MYERS_WINDOW_ALIGNED = 0, MYERS_WINDOW_EXACT = 1 };
+
+/* Kernel path.
+ *  PLAIN: one launch per length bucket present (the fixed-length kernel;
+ *    a single launch when all queries share one bucket).
+ *  BATCHED: one persistent launch pulling length-bucketed work tiles from a
+ *    device queue, replayed from a CUDA graph. */
+enum { MYERS_PATH_PLAIN = 0, MYERS_PATH_BATCHED = 1 };
+
+/* Status-returning versions of the main calls: same behaviour, but errors
+ * are returned instead of ending the process. */
+int myersInit(void ***myersBuffer, uint32_t numBuffers, const char *referenceFileName,
+              int32_t averageQuerySize, int32_t candidatesPerQuery);
+int myersSend(void *myersBuffer, float distance, uint32_t numPEQEntries,
+              uint32_t numQueries, uint32_t numCandidates);
+int myersReceive(void *myersBuffer);
+int myersEnd(void ***myersBuffer);
+
+/* Per-buffer options; take effect at the next send. */
+int myersSetWindowMode(void *myersBuffer, int mode);
+int myersSetKernelPath(void *myersBuffer, int path);
+
+/* Device memory budget (bytes) for all buffers created by the next
+ * initMyers/myersInit, replacing the reference's "95% of free memory"
+ * (src-api/myersGPU.c:323-333). 0 restores the default (the environment
+ * variable MYERS_MEMORY_BUDGET if set, else 4 GiB, capped at 80% of free). */
+int myersSetMemoryBudget(uint64_t bytes);
+
+/* Device of the library's streams (default: the current device at init). */
+int myersGetDevice(void *myersBuffer);
+
+/* Status of the last send/receive of a buffer (sticky until the next send). */
+int myersGetLastStatus(void *myersBuffer);
+
+/* ---------------------------------------------------------------------------
+ * Stream-ordered verification on device-resident inputs
+ * ------------------------------------------------------------------------- */
+
+/* Opaque handle of a packed reference resident in device memory. */
+typedef struct myersReference myersReference_t;
+
+/* Upload `numWords` packed words (the body of a .4bits.ref file) describing
+ * `sizeBases` bases; the library appends N padding. */
+int myersReferenceCreate(myersReference_t **ref, const uint32_t *hostWords, uint64_t numWords,
+                         uint64_t sizeBases);
+/* Load a .4bits.ref file (src-api/genReference-4bits.c:121-140 format). */
+int myersReferenceLoad(myersReference_t **ref, const char *fileName);
+int myersReferenceDestroy(myersReference_t *ref);
+uint64_t myersReferenceSize(const myersReference_t *ref);
+
+/* Opaque per-stream work context: device scratch for length bucketing and
+ * the work queue, sized for up to maxCandidates candidates. */
+typedef struct myersContext myersContext_t;
+int myersContextCreate(myersContext_t **ctx, uint64_t maxCandidates);
+int myersContextDestroy(myersContext_t *ctx);
+
+/* Verify numCandidates candidates on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream). All pointers are device pointers: d_peq
+ * (numPEQEntries qryEntry_t), d_qinfo (numQueries qryInfo_t), d_cands
+ * (numCandidates candInfo_t) and d_results (numCandidates resEntry_t).
+ * Candidates whose window does not fit the reference get {0, 0xFFFFFFFF}.
+ * Asynchronous: returns after enqueueing. */
+int myersVerifyAsync(myersContext_t *ctx, const myersReference_t *ref,
+                     const qryEntry_t *d_peq, uint32_t numPEQEntries,
+                     const qryInfo_t *d_qinfo, uint32_t numQueries,
+                     const candInfo_t *d_cands, uint32_t numCandidates,
+                     float distance, int windowMode, int path,
+                     resEntry_t *d_results, void *stream);
+
+/* As myersVerifyAsync, with the range of query lengths the batch holds
+ * (bases; 0,0 = any). The kernels' shapes are chosen per length bucket; a
+ * narrow range lets the plain path launch only the buckets that can occur
+ * (a single launch, without bucketing, when the range is one bucket).
+ * Queries outside the range get {0, 0xFFFFFFFF} and raise a context flag. */
+int myersVerifyRangeAsync(myersContext_t *ctx, const myersReference_t *ref,
+                          const qryEntry_t *d_peq, uint32_t numPEQEntries,
+                          const qryInfo_t *d_qinfo, uint32_t numQueries,
+                          const candInfo_t *d_cands, uint32_t numCandidates,
+                          float distance, int windowMode, int path,
+                          uint32_t minQuerySize, uint32_t maxQuerySize,
+                          resEntry_t *d_results, void *stream);
+
+/* Kernel launches the last myersVerify*Async on this context enqueued. */
+uint32_t myersContextLastLaunches(const myersContext_t *ctx);
+
+/* Device error flags raised since the last clear (synchronous read):
+ * 1 query too long / window too wide, 2 candidate query index out of range,
+ * 4 query PEQ entries out of range. */
+int myersContextFlags(myersContext_t *ctx, uint32_t *flags, int clear);
+
+/* Kernel launches of a buffer's last send. */
+uint32_t myersBufferLastLaunches(void *myersBuffer);
+
+/* ---------------------------------------------------------------------------
+ * Kernel shapes (autotuning)
+ * ------------------------------------------------------------------------- */
+
+/* Kernel variants: 0..31 one candidate per lane with W = variant+1 words;
+ * 32.. a candidate spread over L lanes of W words. */
+int myersNumVariants(void);
+int myersVariantWords(int variant);
+int myersVariantIsMulti(int variant);
+
+/* Shape the given path uses for a query length. */
+int myersShapeOf(int path, uint32_t querySize, int *variant, int *L, int *W);
+
+/* Force the shape used for queries of `words` 32-bit words
+ * (ceil(size/32)); variant -1 restores the built-in choice. */
+int myersSetShapeOverride(int path, uint32_t words, int variant, int L);
+
+/* Integer-ALU throughput probe on the current device: 3-input logic ops per
+ * second of a device-filling launch (the roofline denominator). */
+int myersProbeIntPeak(double *opsPerSecond, int iters);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MYERS_INTERFACE_H */

@@ -1,0 +1,64 @@
+"""Build the native libraries of the Myers B200 package, in place.
+
+    libmyers_b200.so   CUDA kernels (sm_100a) + host runtime + C ABI
+    libmyers_synth.so  seeded synthetic workload generator (host C, OpenMP)
+
+Run as a script or call build(). nvcc cross-compiles for sm_100a without a
+GPU. Rebuilds only when a source is newer than its library.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CUDA_SOURCES = ["myers_kernels.cu", "myers_api.cu"]
+CUDA_HEADERS = ["myers_internal.h", os.path.join("..", "..", "include", "myers-interface.h")]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_cuda(verbose_ptxas=False):
+    out = os.path.join(HERE, "libmyers_b200.so")
+    srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [__file__]
+    if not _newer(out, deps) and not verbose_ptxas:
+        return out
+    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+           "-I", os.path.join(ROOT, "include"), "-o", out, *srcs]
+    if verbose_ptxas:
+        cmd.insert(1, "-Xptxas=-v")
+    _run(cmd)
+    return out
+
+
+def build_synth():
+    out = os.path.join(HERE, "libmyers_synth.so")
+    src = os.path.join(CSRC, "synth.c")
+    if not _newer(out, [src, __file__]):
+        return out
+    _run(["gcc", "-O3", "-fPIC", "-fopenmp", "-shared", "-o", out, src, "-lm"])
+    return out
+
+
+def build(verbose_ptxas=False):
+    return build_cuda(verbose_ptxas), build_synth()
+
+
+if __name__ == "__main__":
+    build(verbose_ptxas="-v" in sys.argv)

@@ -1,0 +1,739 @@
+// Host runtime and C ABI of libmyers_b200.so.
+//
+// Replaces the reference's host runtime (src-api/myersGPU.c): reference load,
+// per-buffer pinned/device buffers and streams, send/receive, teardown. The
+// differences that matter:
+//  * all buffers live on one device, one stream each (the reference spreads
+//    buffers over devices, myersGPU.c:303-341);
+//  * buffers are sized from a memory budget, not 95% of free memory
+//    (myersGPU.c:323-333);
+//  * length bucketing runs on the device (the reference does three O(C)
+//    passes on the host per send, myersGPU.c:351-422, and un-permutes the
+//    results on the host, :500-513); results land in caller order directly;
+//  * every input index is checked on the device, so malformed buffers give
+//    flagged results instead of out-of-bounds reads;
+//  * errors can be returned (myers*) as well as ending the process (the
+//    reference's calls, which always exit).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/myers-interface.h"
+#include "myers_internal.h"
+
+using namespace myers;
+
+static_assert(sizeof(qryEntry_t) == 80, "qryEntry_t layout");
+static_assert(sizeof(candInfo_t) == 16, "candInfo_t layout");
+static_assert(sizeof(qryInfo_t) == 8, "qryInfo_t layout");
+static_assert(sizeof(resEntry_t) == 8, "resEntry_t layout");
+static_assert(sizeof(Cand) == 16, "Cand layout");
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local char g_cuda_msg[256];
+
+static int cuda_fail(cudaError_t e, const char* what) {
+  snprintf(g_cuda_msg, sizeof(g_cuda_msg), "%s: %s", what, cudaGetErrorString(e));
+  return MYERS_E_CUDA;
+}
+
+#define CU(call)                                   \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+extern "C" const char* myersGetErrorString(int status) {
+  switch (status) {
+    case MYERS_SUCCESS: return "Myers - Success";
+    case MYERS_E_OPENING_FILE: return "Myers - Error: opening file";
+    case MYERS_E_READING_FILE: return "Myers - Error: reading file";
+    case MYERS_E_INSUFFICIENT_MEM_GPU: return "Myers - Error: there aren't enough GPU memory space";
+    case MYERS_E_ALLOCATE_MEM: return "Myers - Error: allocating data";
+    case MYERS_E_INCOMPATIBLE_GPU: return "Myers - Error: incompatible GPU (needs compute capability 10.0)";
+    case MYERS_E_INVALID_ARGUMENT: return "Myers - Error: invalid argument";
+    case MYERS_E_CAPACITY: return "Myers - Error: more data than the buffer holds";
+    case MYERS_E_QUERY_TOO_LONG: return "Myers - Error: query or window too long, or invalid query/PEQ indices";
+    case MYERS_E_CUDA: return g_cuda_msg[0] ? g_cuda_msg : "Myers - Error: CUDA runtime call failed";
+    case MYERS_E_TIMEOUT: return "Myers - Error: device wait timed out";
+    case MYERS_E_NOT_READY: return "Myers - Error: not ready";
+    case MYERS_E_BUSY: return "Myers - Error: busy";
+    default: return "Myers - Unknown error";
+  }
+}
+
+// The reference's convention: print and end the process (myersGPU.c:24-47).
+static void fatal(int status, const char* where) {
+  if (status != MYERS_SUCCESS) {
+    fprintf(stderr, "%s in %s\n", myersGetErrorString(status), where);
+    exit(EXIT_FAILURE);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// reference
+
+struct myersReference {
+  int device;
+  uint32_t* d_words;
+  uint64_t words;  // packed words (without padding)
+  uint64_t size;   // bases
+};
+
+static int reference_upload(myersReference** out, const uint32_t* host, uint64_t words, uint64_t size) {
+  if (out == nullptr || (words > 0 && host == nullptr)) return MYERS_E_INVALID_ARGUMENT;
+  if (size > words * 8) return MYERS_E_INVALID_ARGUMENT;
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  int major = 0;
+  CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (major < 10) return MYERS_E_INCOMPATIBLE_GPU;
+  size_t freeb = 0, totalb = 0;
+  CU(cudaMemGetInfo(&freeb, &totalb));
+  const uint64_t bytes = (words + kRefPadWords) * 4;
+  if (bytes > freeb) return MYERS_E_INSUFFICIENT_MEM_GPU;
+  myersReference* r = new myersReference();
+  r->device = dev;
+  r->words = words;
+  r->size = size;
+  if (cudaMalloc((void**)&r->d_words, bytes) != cudaSuccess) {
+    delete r;
+    return MYERS_E_INSUFFICIENT_MEM_GPU;
+  }
+  cudaError_t e = cudaMemcpy(r->d_words, host, words * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    std::vector<uint32_t> pad(kRefPadWords, kPadWord);
+    e = cudaMemcpy(r->d_words + words, pad.data(), kRefPadWords * 4, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(r->d_words);
+    delete r;
+    return cuda_fail(e, "reference upload");
+  }
+  *out = r;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersReferenceCreate(myersReference_t** ref, const uint32_t* hostWords, uint64_t numWords,
+                                    uint64_t sizeBases) {
+  return reference_upload(ref, hostWords, numWords, sizeBases);
+}
+
+// File format of src-api/genReference-4bits.c:121-140: u32 numEntries,
+// u32 size, then numEntries packed words (read at src-api/myersGPU.c:106-128).
+extern "C" int myersReferenceLoad(myersReference_t** ref, const char* fileName) {
+  if (ref == nullptr || fileName == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  FILE* fp = fopen(fileName, "rb");
+  if (fp == nullptr) return MYERS_E_OPENING_FILE;
+  uint32_t hdr[2];
+  if (fread(hdr, sizeof(uint32_t), 2, fp) != 2) {
+    fclose(fp);
+    return MYERS_E_READING_FILE;
+  }
+  uint32_t* host = nullptr;
+  if (cudaMallocHost((void**)&host, (size_t)hdr[0] * 4 + 4) != cudaSuccess) {
+    fclose(fp);
+    return MYERS_E_ALLOCATE_MEM;
+  }
+  size_t got = fread(host, sizeof(uint32_t), hdr[0], fp);
+  fclose(fp);
+  int st = MYERS_E_READING_FILE;
+  if (got == hdr[0]) st = reference_upload(ref, host, hdr[0], hdr[1]);
+  cudaFreeHost(host);
+  return st;
+}
+
+extern "C" int myersReferenceDestroy(myersReference_t* ref) {
+  if (ref == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(ref->device);
+  cudaFree(ref->d_words);
+  cudaSetDevice(cur);
+  delete ref;
+  return MYERS_SUCCESS;
+}
+
+extern "C" uint64_t myersReferenceSize(const myersReference_t* ref) { return ref ? ref->size : 0; }
+
+// ---------------------------------------------------------------------------
+// shapes and plans
+
+// Lanes a candidate effectively occupies (a warp holds floor(32/L)
+// candidates) times the instructions of one column step per lane.
+static double shape_cost(int v, int L) {
+  const int W = variant_W(v);
+  if (!variant_multi(v)) return 10.0 * W + 8.0;
+  const int nseg = 32 / L;
+  return (32.0 / nseg) * (10.0 * W + 16.0);
+}
+
+// Optional per-word-count overrides (variant, L) set by the autotuner.
+struct Override {
+  bool set;
+  uint8_t variant;
+  uint8_t L;
+};
+static std::mutex g_override_mu;
+static Override g_override[2][kMaxWords + 1];
+
+static Shape pick_shape(uint32_t w, bool batched) {
+  {
+    std::lock_guard<std::mutex> lk(g_override_mu);
+    const Override& o = g_override[batched ? 1 : 0][w];
+    if (o.set) return Shape{o.variant, o.L, (uint8_t)variant_W(o.variant), 0};
+  }
+  const uint32_t single_max = batched ? (uint32_t)kBatchedMaxW : 32u;
+  if (w <= single_max) return Shape{(uint8_t)(w - 1), 1, (uint8_t)w, 0};
+  double best = 1e300;
+  Shape bs{0, 0, 0, 0};
+  for (int mi = 0; mi < kNumMulti; ++mi) {
+    const int W = kMultiW[mi];
+    const uint32_t L = (w + W - 1) / W;
+    if (L < 2 || L > 32) continue;
+    const double c = shape_cost(kNumSingle + mi, (int)L);
+    // batched shapes that the persistent kernel cannot carry cost extra
+    const double pen = (batched && W > kBatchedMaxW) ? 4.0 : 1.0;
+    if (c * pen < best) {
+      best = c * pen;
+      bs = Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};
+    }
+  }
+  return bs;
+}
+
+// Build the plan for the word counts flagged in `present` (size kMaxWords+1).
+static int build_plan(PlanTable& t, const uint8_t* present, bool batched) {
+  memset(&t, 0, sizeof(t));
+  memset(t.cfg_of_words, kNoCfg, sizeof(t.cfg_of_words));
+  struct Entry {
+    Shape s;
+    uint32_t max_words;
+  };
+  std::vector<Entry> shapes;
+  std::vector<int> cfg_of(kMaxWords + 1, -1);
+  for (uint32_t w = 1; w <= kMaxWords; ++w) {
+    if (!present[w]) continue;
+    const Shape s = pick_shape(w, batched);
+    if (s.L == 0) return MYERS_E_QUERY_TOO_LONG;
+    int found = -1;
+    for (size_t i = 0; i < shapes.size(); ++i)
+      if (shapes[i].s.variant == s.variant && shapes[i].s.L == s.L) found = (int)i;
+    if (found < 0) {
+      shapes.push_back(Entry{s, w});
+      found = (int)shapes.size() - 1;
+    }
+    if (w > shapes[found].max_words) shapes[found].max_words = w;
+    cfg_of[w] = found;
+  }
+  if (shapes.size() > (size_t)kMaxCfg) return MYERS_E_QUERY_TOO_LONG;
+  // order: persistent-kernel shapes first, each group by decreasing cost
+  std::vector<int> order(shapes.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  auto key = [&](int i) {
+    const bool b = batched_supports(shapes[i].s.variant);
+    const double cost = shape_cost(shapes[i].s.variant, shapes[i].s.L) * shapes[i].max_words;
+    return std::make_pair(b ? 0 : 1, -cost);
+  };
+  for (size_t i = 1; i < order.size(); ++i)
+    for (size_t j = i; j > 0 && key(order[j]) < key(order[j - 1]); --j) std::swap(order[j], order[j - 1]);
+  std::vector<int> rank(shapes.size());
+  t.num_cfg = (uint32_t)shapes.size();
+  t.num_batched = 0;
+  for (size_t r = 0; r < order.size(); ++r) {
+    rank[order[r]] = (int)r;
+    t.shape[r] = shapes[order[r]].s;
+    if (batched_supports(t.shape[r].variant)) t.num_batched = (uint32_t)r + 1;
+  }
+  for (uint32_t w = 1; w <= kMaxWords; ++w)
+    if (cfg_of[w] >= 0) t.cfg_of_words[w] = (uint8_t)rank[cfg_of[w]];
+  return MYERS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// context: device scratch for bucketing
+
+struct myersContext {
+  int device;
+  int num_sms;
+  uint64_t capacity;
+  uint32_t* d_ids;
+  uint8_t* d_cfg;
+  BucketState* d_state;
+  uint32_t* d_flags;
+  uint32_t last_launches;
+};
+
+extern "C" int myersContextCreate(myersContext_t** out, uint64_t maxCandidates) {
+  if (out == nullptr || maxCandidates > 0xFFFFFFFFull) return MYERS_E_INVALID_ARGUMENT;
+  myersContext* c = new myersContext();
+  memset(c, 0, sizeof(*c));
+  cudaError_t e = cudaGetDevice(&c->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  c->capacity = maxCandidates;
+  const size_t n = maxCandidates ? maxCandidates : 1;
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_ids, n * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cfg, n);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_state, sizeof(BucketState));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_flags, 4);
+  if (e == cudaSuccess) e = cudaMemset(c->d_flags, 0, 4);
+  if (e != cudaSuccess) {
+    cudaFree(c->d_ids);
+    cudaFree(c->d_cfg);
+    cudaFree(c->d_state);
+    cudaFree(c->d_flags);
+    delete c;
+    return e == cudaErrorMemoryAllocation ? MYERS_E_INSUFFICIENT_MEM_GPU : cuda_fail(e, "context");
+  }
+  *out = c;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersContextDestroy(myersContext_t* c) {
+  if (c == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(c->device);
+  cudaFree(c->d_ids);
+  cudaFree(c->d_cfg);
+  cudaFree(c->d_state);
+  cudaFree(c->d_flags);
+  cudaSetDevice(cur);
+  delete c;
+  return MYERS_SUCCESS;
+}
+
+extern "C" uint32_t myersContextLastLaunches(const myersContext_t* c) { return c ? c->last_launches : 0; }
+
+// Enqueue the kernels for one batch. `uniform`: every query maps to the same
+// (single) shape of `plan`, so no bucketing is needed on the plain path.
+static int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in0, const PlanTable& plan,
+                          int path, cudaStream_t s) {
+  DevInputs in = in0;
+  in.ref = ref->d_words;
+  in.ref_size = ref->size;
+  in.ref_words = ref->words + kRefPadWords;
+  in.flags = ctx->d_flags;
+  ctx->last_launches = 0;
+  if (in.num_cands == 0) return MYERS_SUCCESS;
+  if (in.num_cands > ctx->capacity) return MYERS_E_CAPACITY;
+  if (plan.num_cfg == 0) {
+    // no query needs the DP (all empty or all too long): classify alone
+    // writes every result
+  }
+  if (path == MYERS_PATH_PLAIN && plan.num_cfg == 1) {
+    const Shape sh = plan.shape[0];
+    CU(launch_plain(sh.variant, sh.L, in, nullptr, nullptr, 0, 0, in.num_cands, s, ctx->num_sms));
+    ctx->last_launches = 1;
+    return MYERS_SUCCESS;
+  }
+  CU(cudaMemsetAsync(ctx->d_state, 0, sizeof(BucketState), s));
+  cudaError_t e = cudaSuccess;
+  uint32_t launches = (uint32_t)launch_bucketing(in, plan, ctx->d_state, ctx->d_cfg, ctx->d_ids, s, ctx->num_sms, &e);
+  if (e != cudaSuccess) return cuda_fail(e, "bucketing");
+  uint32_t first_plain = 0;
+  if (path == MYERS_PATH_BATCHED && plan.num_batched > 0) {
+    CU(launch_batched(in, ctx->d_ids, plan, ctx->d_state, s, ctx->num_sms));
+    ++launches;
+    first_plain = plan.num_batched;
+  }
+  for (uint32_t c = first_plain; c < plan.num_cfg; ++c) {
+    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, ctx->d_ids, ctx->d_state, (int)c, 0, 0, s,
+                    ctx->num_sms));
+    ++launches;
+  }
+  ctx->last_launches = launches;
+  return MYERS_SUCCESS;
+}
+
+static int plan_for_range(PlanTable& plan, uint32_t minSize, uint32_t maxSize, int path) {
+  std::vector<uint8_t> present(kMaxWords + 1, 0);
+  if (maxSize == 0) maxSize = kMaxWords * 32;
+  if (maxSize > kMaxWords * 32) maxSize = kMaxWords * 32;
+  const uint32_t wlo = minSize ? (minSize + 31) / 32 : 1, whi = (maxSize + 31) / 32;
+  for (uint32_t w = wlo; w <= whi; ++w) present[w] = 1;
+  return build_plan(plan, present.data(), path == MYERS_PATH_BATCHED);
+}
+
+extern "C" int myersVerifyAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
+                                uint32_t numPEQEntries, const qryInfo_t* d_qinfo, uint32_t numQueries,
+                                const candInfo_t* d_cands, uint32_t numCandidates, float distance,
+                                int windowMode, int path, resEntry_t* d_results, void* stream) {
+  return myersVerifyRangeAsync(ctx, ref, d_peq, numPEQEntries, d_qinfo, numQueries, d_cands, numCandidates,
+                               distance, windowMode, path, 0, 0, d_results, stream);
+}
+
+extern "C" int myersVerifyRangeAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
+                                     uint32_t numPEQEntries, const qryInfo_t* d_qinfo, uint32_t numQueries,
+                                     const candInfo_t* d_cands, uint32_t numCandidates, float distance,
+                                     int windowMode, int path, uint32_t minQuerySize, uint32_t maxQuerySize,
+                                     resEntry_t* d_results, void* stream) {
+  if (ctx == nullptr || ref == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  if (!(distance >= 0.0f) || !std::isfinite(distance)) return MYERS_E_INVALID_ARGUMENT;
+  if (windowMode != MYERS_WINDOW_ALIGNED && windowMode != MYERS_WINDOW_EXACT) return MYERS_E_INVALID_ARGUMENT;
+  if (path != MYERS_PATH_PLAIN && path != MYERS_PATH_BATCHED) return MYERS_E_INVALID_ARGUMENT;
+  if (numCandidates > 0 && (d_peq == nullptr || d_qinfo == nullptr || d_cands == nullptr || d_results == nullptr))
+    return MYERS_E_INVALID_ARGUMENT;
+  PlanTable plan;
+  int st = plan_for_range(plan, minQuerySize, maxQuerySize, path);
+  if (st != MYERS_SUCCESS) return st;
+  DevInputs in;
+  memset(&in, 0, sizeof(in));
+  in.peq = reinterpret_cast<const uint32_t*>(d_peq);
+  in.qinfo = reinterpret_cast<const uint2*>(d_qinfo);
+  in.cands = reinterpret_cast<const Cand*>(d_cands);
+  in.results = reinterpret_cast<uint2*>(d_results);
+  in.num_cands = numCandidates;
+  in.num_queries = numQueries;
+  in.num_entries = numPEQEntries;
+  in.distance = distance;
+  in.exact = windowMode == MYERS_WINDOW_EXACT;
+  return verify_enqueue(ctx, ref, in, plan, path, (cudaStream_t)stream);
+}
+
+extern "C" int myersContextFlags(myersContext_t* ctx, uint32_t* flags, int clear) {
+  if (ctx == nullptr || flags == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  CU(cudaMemcpy(flags, ctx->d_flags, 4, cudaMemcpyDeviceToHost));
+  if (clear) CU(cudaMemset(ctx->d_flags, 0, 4));
+  return MYERS_SUCCESS;
+}
+
+// Autotuner hook: force the shape of one word count (variant, L); variant
+// -1 clears the override.
+extern "C" int myersSetShapeOverride(int path, uint32_t words, int variant, int L) {
+  if ((path != MYERS_PATH_PLAIN && path != MYERS_PATH_BATCHED) || words == 0 || words > kMaxWords)
+    return MYERS_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(g_override_mu);
+  Override& o = g_override[path][words];
+  if (variant < 0) {
+    o.set = false;
+    return MYERS_SUCCESS;
+  }
+  if (variant >= kNumVariants) return MYERS_E_INVALID_ARGUMENT;
+  if (!variant_multi(variant)) L = 1;
+  if (L < 1 || L > 32 || (uint32_t)(variant_W(variant) * L) < words) return MYERS_E_INVALID_ARGUMENT;
+  if (path == MYERS_PATH_BATCHED && variant_multi(variant) == false && !batched_supports(variant))
+    return MYERS_E_INVALID_ARGUMENT;
+  o.set = true;
+  o.variant = (uint8_t)variant;
+  o.L = (uint8_t)L;
+  return MYERS_SUCCESS;
+}
+
+// Shape the plan would use for a query length (for tests and the autotuner).
+extern "C" int myersShapeOf(int path, uint32_t querySize, int* variant, int* L, int* W) {
+  if (querySize == 0 || querySize > kMaxWords * 32 || variant == nullptr || L == nullptr || W == nullptr)
+    return MYERS_E_INVALID_ARGUMENT;
+  const Shape s = pick_shape((querySize + 31) / 32, path == MYERS_PATH_BATCHED);
+  *variant = s.variant;
+  *L = s.L;
+  *W = s.W;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersNumVariants(void) { return kNumVariants; }
+extern "C" int myersVariantWords(int v) { return (v >= 0 && v < kNumVariants) ? variant_W(v) : -1; }
+extern "C" int myersVariantIsMulti(int v) { return (v >= 0 && v < kNumVariants) ? (int)variant_multi(v) : -1; }
+
+// Integer-ALU probe: returns 3-input logic ops executed per second by a
+// device-filling launch (timed with CUDA events on the given stream).
+extern "C" int myersProbeIntPeak(double* opsPerSecond, int iters) {
+  if (opsPerSecond == nullptr || iters <= 0) return MYERS_E_INVALID_ARGUMENT;
+  int dev = 0, sms = 0;
+  CU(cudaGetDevice(&dev));
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int threads = 256, blocks = sms * 8;
+  uint32_t* d_out = nullptr;
+  CU(cudaMalloc((void**)&d_out, (size_t)blocks * threads * 4));
+  cudaEvent_t a, b;
+  CU(cudaEventCreate(&a));
+  CU(cudaEventCreate(&b));
+  CU(launch_lop3_probe(d_out, blocks, threads, 2, nullptr));  // warm-up
+  CU(cudaEventRecord(a, nullptr));
+  CU(launch_lop3_probe(d_out, blocks, threads, iters, nullptr));
+  CU(cudaEventRecord(b, nullptr));
+  CU(cudaEventSynchronize(b));
+  float ms = 0.f;
+  CU(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d_out);
+  const double ops = (double)blocks * threads * iters * 16.0 * 8.0;
+  *opsPerSecond = ops / (ms * 1e-3);
+  return MYERS_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// drop-in buffers (the reference's buffer_t, src-api/myers-common.h:129-145)
+
+static std::mutex g_budget_mu;
+static uint64_t g_budget = 0;
+
+extern "C" int myersSetMemoryBudget(uint64_t bytes) {
+  std::lock_guard<std::mutex> lk(g_budget_mu);
+  g_budget = bytes;
+  return MYERS_SUCCESS;
+}
+
+static uint64_t budget_bytes(uint64_t freeb) {
+  uint64_t b;
+  {
+    std::lock_guard<std::mutex> lk(g_budget_mu);
+    b = g_budget;
+  }
+  if (b == 0) {
+    const char* env = getenv("MYERS_MEMORY_BUDGET");
+    b = env ? strtoull(env, nullptr, 10) : 0;
+  }
+  if (b == 0) b = 4ull << 30;
+  const uint64_t cap = (uint64_t)(freeb * 0.8);
+  return b < cap ? b : cap;
+}
+
+struct Shared {
+  myersReference* ref;
+  uint32_t refs;  // buffers still holding it
+};
+
+struct Buffer {
+  uint32_t numBuffers;
+  uint32_t idBuffer;
+  uint32_t maxPEQEntries, maxCandidates, maxQueries;
+  int device;
+  cudaStream_t stream;
+  Shared* shared;
+  myersContext* ctx;
+  qryEntry_t* h_peq;
+  qryInfo_t* h_qinfo;
+  candInfo_t* h_cands;
+  resEntry_t* h_results;
+  uint32_t* h_flags;
+  qryEntry_t* d_peq;
+  qryInfo_t* d_qinfo;
+  candInfo_t* d_cands;
+  resEntry_t* d_results;
+  int window_mode;
+  int path;
+  int last_status;
+  bool pending;
+  std::vector<uint8_t> present;  // word counts of the last send
+  PlanTable plan;
+  bool plan_valid;
+  int plan_path;
+};
+
+extern "C" qryEntry_t* getPEQBuffer(void* b) { return b ? static_cast<Buffer*>(b)->h_peq : nullptr; }
+extern "C" candInfo_t* getCandidatesBuffer(void* b) { return b ? static_cast<Buffer*>(b)->h_cands : nullptr; }
+extern "C" qryInfo_t* getPEQInfoBuffer(void* b) { return b ? static_cast<Buffer*>(b)->h_qinfo : nullptr; }
+extern "C" resEntry_t* getResultsBuffer(void* b) { return b ? static_cast<Buffer*>(b)->h_results : nullptr; }
+extern "C" uint32_t getMaxPEQEntries(void* b) { return b ? static_cast<Buffer*>(b)->maxPEQEntries : 0; }
+extern "C" uint32_t getMaxCandidates(void* b) { return b ? static_cast<Buffer*>(b)->maxCandidates : 0; }
+extern "C" uint32_t getMaxQueries(void* b) { return b ? static_cast<Buffer*>(b)->maxQueries : 0; }
+
+static void buffer_free(Buffer* b) {
+  if (b == nullptr) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  cudaFreeHost(b->h_peq);
+  cudaFreeHost(b->h_qinfo);
+  cudaFreeHost(b->h_cands);
+  cudaFreeHost(b->h_results);
+  cudaFreeHost(b->h_flags);
+  cudaFree(b->d_peq);
+  cudaFree(b->d_qinfo);
+  cudaFree(b->d_cands);
+  cudaFree(b->d_results);
+  if (b->ctx) myersContextDestroy(b->ctx);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->shared && --b->shared->refs == 0) {
+    myersReferenceDestroy(b->shared->ref);
+    delete b->shared;
+  }
+  delete b;
+}
+
+static int buffer_alloc(Buffer* b) {
+#define ALLOC_H(p, n) \
+  if (cudaHostAlloc((void**)&(p), (size_t)(n) ? (size_t)(n) : 1, cudaHostAllocDefault) != cudaSuccess) return MYERS_E_ALLOCATE_MEM
+#define ALLOC_D(p, n) \
+  if (cudaMalloc((void**)&(p), (size_t)(n) ? (size_t)(n) : 1) != cudaSuccess) return MYERS_E_INSUFFICIENT_MEM_GPU
+  CU(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  ALLOC_H(b->h_peq, (size_t)b->maxPEQEntries * sizeof(qryEntry_t));
+  ALLOC_H(b->h_qinfo, (size_t)b->maxQueries * sizeof(qryInfo_t));
+  ALLOC_H(b->h_cands, (size_t)b->maxCandidates * sizeof(candInfo_t));
+  ALLOC_H(b->h_results, (size_t)b->maxCandidates * sizeof(resEntry_t));
+  ALLOC_H(b->h_flags, 4);
+  ALLOC_D(b->d_peq, (size_t)b->maxPEQEntries * sizeof(qryEntry_t));
+  ALLOC_D(b->d_qinfo, (size_t)b->maxQueries * sizeof(qryInfo_t));
+  ALLOC_D(b->d_cands, (size_t)b->maxCandidates * sizeof(candInfo_t));
+  ALLOC_D(b->d_results, (size_t)b->maxCandidates * sizeof(resEntry_t));
+#undef ALLOC_H
+#undef ALLOC_D
+  return myersContextCreate(&b->ctx, b->maxCandidates);
+}
+
+extern "C" int myersInit(void*** myersBuffer, uint32_t numBuffers, const char* referenceFileName,
+                         int32_t averageQuerySize, int32_t candidatesPerQuery) {
+  if (myersBuffer == nullptr || numBuffers == 0 || referenceFileName == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  // defaults of src-api/myersGPU.c:300-301
+  if (averageQuerySize <= 0) averageQuerySize = 1024;
+  if (candidatesPerQuery <= 0) candidatesPerQuery = 1;
+  myersReference* ref = nullptr;
+  int st = myersReferenceLoad(&ref, referenceFileName);
+  if (st != MYERS_SUCCESS) return st;
+  Shared* shared = new Shared{ref, 0};
+  size_t freeb = 0, totalb = 0;
+  CU(cudaMemGetInfo(&freeb, &totalb));
+  // sizing as src-api/myersGPU.c:312-330, over the budget instead of free memory
+  const uint32_t entries_per_query = (averageQuerySize + NUM_BASES_ENTRY - 1) / NUM_BASES_ENTRY;
+  const double bytes_per_cand = (entries_per_query * sizeof(qryEntry_t) + sizeof(qryInfo_t)) / (double)candidatesPerQuery +
+                                sizeof(candInfo_t) + sizeof(resEntry_t) + sizeof(uint32_t) + 1.0;
+  const uint64_t per_buffer = budget_bytes(freeb) / numBuffers;
+  uint64_t max_cands = (uint64_t)(per_buffer / bytes_per_cand);
+  if (max_cands > 0x7FFFFFFFull) max_cands = 0x7FFFFFFFull;
+  uint64_t max_queries = max_cands / (uint32_t)candidatesPerQuery;
+  uint64_t max_entries = max_queries * entries_per_query;
+  if (max_cands < 1 || max_queries < 1 || max_entries > 0xFFFFFFFFull) {
+    myersReferenceDestroy(ref);
+    delete shared;
+    return MYERS_E_INSUFFICIENT_MEM_GPU;
+  }
+  Buffer** bufs = (Buffer**)calloc(numBuffers, sizeof(Buffer*));
+  if (bufs == nullptr) return MYERS_E_ALLOCATE_MEM;
+  for (uint32_t i = 0; i < numBuffers; ++i) {
+    Buffer* b = new Buffer();
+    b->numBuffers = numBuffers;
+    b->idBuffer = i;
+    b->maxCandidates = (uint32_t)max_cands;
+    b->maxQueries = (uint32_t)max_queries;
+    b->maxPEQEntries = (uint32_t)max_entries;
+    b->device = ref->device;
+    b->shared = shared;
+    shared->refs++;
+    b->window_mode = MYERS_WINDOW_ALIGNED;
+    b->path = MYERS_PATH_PLAIN;
+    const char* p = getenv("MYERS_PATH");
+    if (p && strcmp(p, "batched") == 0) b->path = MYERS_PATH_BATCHED;
+    b->present.assign(kMaxWords + 1, 0);
+    bufs[i] = b;
+    st = buffer_alloc(b);
+    if (st != MYERS_SUCCESS) {
+      for (uint32_t j = 0; j <= i; ++j) buffer_free(bufs[j]);
+      free(bufs);
+      return st;
+    }
+  }
+  *myersBuffer = (void**)bufs;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int initMyers(void*** myersBuffer, uint32_t numBuffers, const char* referenceFileName,
+                         int32_t averageQuerySize, int32_t candidatesPerQuery) {
+  fatal(myersInit(myersBuffer, numBuffers, referenceFileName, averageQuerySize, candidatesPerQuery), "initMyers");
+  return 0;
+}
+
+extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint32_t numQueries,
+                         uint32_t numCandidates) {
+  Buffer* b = static_cast<Buffer*>(mb);
+  if (b == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  b->last_status = MYERS_SUCCESS;
+  if (!(distance >= 0.0f) || !std::isfinite(distance)) return b->last_status = MYERS_E_INVALID_ARGUMENT;
+  if (numPEQEntries > b->maxPEQEntries || numQueries > b->maxQueries || numCandidates > b->maxCandidates)
+    return b->last_status = MYERS_E_CAPACITY;
+  CU(cudaSetDevice(b->device));
+  // O(queries) host pass: the word counts present pick the shapes
+  std::vector<uint8_t>& present = b->present;
+  std::fill(present.begin(), present.end(), 0);
+  bool too_long = false;
+  for (uint32_t q = 0; q < numQueries; ++q) {
+    const uint32_t m = b->h_qinfo[q].size;
+    if (m > kMaxWords * 32) too_long = true;
+    else if (m > 0) present[(m + 31) / 32] = 1;
+  }
+  (void)too_long;  // flagged on the device per candidate
+  PlanTable& plan = b->plan;
+  int st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
+  if (st != MYERS_SUCCESS) return b->last_status = st;
+  cudaStream_t s = b->stream;
+  CU(cudaMemsetAsync(b->ctx->d_flags, 0, 4, s));
+  CU(cudaMemcpyAsync(b->d_peq, b->h_peq, (size_t)numPEQEntries * sizeof(qryEntry_t), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(b->d_qinfo, b->h_qinfo, (size_t)numQueries * sizeof(qryInfo_t), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(b->d_cands, b->h_cands, (size_t)numCandidates * sizeof(candInfo_t), cudaMemcpyHostToDevice, s));
+  DevInputs in;
+  memset(&in, 0, sizeof(in));
+  in.peq = reinterpret_cast<const uint32_t*>(b->d_peq);
+  in.qinfo = reinterpret_cast<const uint2*>(b->d_qinfo);
+  in.cands = reinterpret_cast<const Cand*>(b->d_cands);
+  in.results = reinterpret_cast<uint2*>(b->d_results);
+  in.num_cands = numCandidates;
+  in.num_queries = numQueries;
+  in.num_entries = numPEQEntries;
+  in.distance = distance;
+  in.exact = b->window_mode == MYERS_WINDOW_EXACT;
+  st = verify_enqueue(b->ctx, b->shared->ref, in, plan, b->path, s);
+  if (st != MYERS_SUCCESS) return b->last_status = st;
+  CU(cudaMemcpyAsync(b->h_results, b->d_results, (size_t)numCandidates * sizeof(resEntry_t), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(b->h_flags, b->ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
+  b->pending = true;
+  return MYERS_SUCCESS;
+}
+
+extern "C" void sendMyersBuffer(void* mb, float distance, uint32_t numPEQEntries, uint32_t numQueries,
+                                uint32_t numCandidates) {
+  fatal(myersSend(mb, distance, numPEQEntries, numQueries, numCandidates), "sendMyersBuffer");
+}
+
+extern "C" int myersReceive(void* mb) {
+  Buffer* b = static_cast<Buffer*>(mb);
+  if (b == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  CU(cudaSetDevice(b->device));
+  CU(cudaStreamSynchronize(b->stream));
+  if (b->pending) {
+    b->pending = false;
+    if (*b->h_flags != 0) b->last_status = MYERS_E_QUERY_TOO_LONG;
+  }
+  return b->last_status;
+}
+
+extern "C" void receiveMyersBuffer(void* mb) { fatal(myersReceive(mb), "receiveMyersBuffer"); }
+
+extern "C" int myersEnd(void*** myersBuffer) {
+  if (myersBuffer == nullptr || *myersBuffer == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  Buffer** bufs = (Buffer**)(*myersBuffer);
+  const uint32_t n = bufs[0]->numBuffers;
+  for (uint32_t i = 0; i < n; ++i) buffer_free(bufs[i]);
+  free(bufs);
+  *myersBuffer = nullptr;
+  return MYERS_SUCCESS;
+}
+
+extern "C" void endMyers(void*** myersBuffer) { fatal(myersEnd(myersBuffer), "endMyers"); }
+
+extern "C" int myersSetWindowMode(void* mb, int mode) {
+  Buffer* b = static_cast<Buffer*>(mb);
+  if (b == nullptr || (mode != MYERS_WINDOW_ALIGNED && mode != MYERS_WINDOW_EXACT)) return MYERS_E_INVALID_ARGUMENT;
+  b->window_mode = mode;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersSetKernelPath(void* mb, int path) {
+  Buffer* b = static_cast<Buffer*>(mb);
+  if (b == nullptr || (path != MYERS_PATH_PLAIN && path != MYERS_PATH_BATCHED)) return MYERS_E_INVALID_ARGUMENT;
+  b->path = path;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersGetDevice(void* mb) { return mb ? static_cast<Buffer*>(mb)->device : -1; }
+extern "C" int myersGetLastStatus(void* mb) { return mb ? static_cast<Buffer*>(mb)->last_status : MYERS_E_INVALID_ARGUMENT; }
+extern "C" uint32_t myersBufferLastLaunches(void* mb) {
+  return mb ? static_cast<Buffer*>(mb)->ctx->last_launches : 0;
+}

@@ -1,0 +1,119 @@
+// Internal types shared by the kernels (myers_kernels.cu) and the host
+// runtime (myers_api.cu). Not part of the public ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace myers {
+
+// Eight N codes: what the kernels read past the end of the packed reference.
+constexpr uint32_t kPadWord = 0x44444444u;
+// Words of N padding appended to the device copy of the reference, so the
+// window reads past the last packed word stay inside the allocation.
+constexpr uint64_t kRefPadWords = 64;
+constexpr uint32_t kNoResult = 0xFFFFFFFFu;
+constexpr uint32_t kMaxWords = 1024;          // 32768 bases
+constexpr uint32_t kMaxColumns = 65535;       // the result key keeps 16 column bits
+
+// Device error flags (BucketState::flags / DevInputs::flags).
+constexpr uint32_t kFlagUnsupported = 1u;     // query too long or window too wide
+constexpr uint32_t kFlagBadQuery = 2u;        // candidate query index >= numQueries
+constexpr uint32_t kFlagBadEntry = 4u;        // query PEQ entries beyond numPEQEntries
+
+// Candidate as laid out by the API (candInfo_t with its 4 padding bytes).
+struct Cand {
+  uint32_t query;
+  uint32_t pad;
+  unsigned long long position;
+};
+
+// Kernel variants. Single-lane variants (one candidate per lane, W words of
+// 32 query rows each) cover W = 1..32; multi-lane variants spread one
+// candidate over L lanes of W words and hand the horizontal delta from lane
+// to lane once per column.
+constexpr int kNumSingle = 32;
+constexpr int kMultiW[] = {4, 6, 8, 10, 12, 16, 32};
+constexpr int kNumMulti = sizeof(kMultiW) / sizeof(kMultiW[0]);
+constexpr int kNumVariants = kNumSingle + kNumMulti;
+// The persistent kernel carries single W <= 16 and multi W <= 16.
+constexpr int kBatchedMaxW = 16;
+
+// A length bucket's launch shape: variant (kernel template), lanes per
+// candidate L and words per lane W. Buckets are indexed by the number of
+// 32-bit query words, ceil(m/32).
+struct Shape {
+  uint8_t variant;  // 0..31 single W=variant+1; 32.. multi kMultiW[variant-32]
+  uint8_t L;
+  uint8_t W;
+  uint8_t pad;
+};
+
+constexpr int kMaxCfg = 128;            // distinct shapes in one plan
+constexpr uint8_t kNoCfg = 0xFF;
+
+// Per-send plan, passed by value as a __grid_constant__ kernel parameter:
+// word count -> shape index, and the shapes in launch order. The first
+// num_batched shapes (most expensive first) go to the persistent kernel on
+// the batched path; the rest always get plain launches.
+struct PlanTable {
+  uint8_t cfg_of_words[kMaxWords + 1];
+  uint8_t pad[3];
+  uint32_t num_cfg;
+  uint32_t num_batched;
+  Shape shape[kMaxCfg];
+};
+
+// Device-computed layout of the bucketed candidate list.
+struct BucketState {
+  uint32_t count[kMaxCfg];       // candidates per shape
+  uint32_t first[kMaxCfg];       // first slot in the sorted id array
+  uint32_t cursor[kMaxCfg];      // scatter cursors
+  uint32_t tile_start[kMaxCfg + 1];
+  uint32_t total_tiles;          // tiles of the first num_batched shapes
+  uint32_t queue;                // persistent kernel work counter
+  uint32_t pad[2];
+};
+
+struct DevInputs {
+  const uint32_t* peq;           // qryEntry_t as 20 u32
+  const uint2* qinfo;            // {posEntry, size}
+  const Cand* cands;
+  const uint32_t* ref;           // packed reference words
+  unsigned long long ref_size;   // bases
+  unsigned long long ref_words;  // readable words (packed + padding)
+  uint2* results;                // {column, score}
+  uint32_t* flags;               // device error flags (kFlag*)
+  uint32_t num_cands;
+  uint32_t num_queries;
+  uint32_t num_entries;
+  float distance;
+  int exact;
+};
+
+inline int variant_W(int v) { return v < kNumSingle ? v + 1 : kMultiW[v - kNumSingle]; }
+inline bool variant_multi(int v) { return v >= kNumSingle; }
+inline bool batched_supports(int v) { return variant_W(v) <= kBatchedMaxW; }
+
+// ---- host launchers (myers_kernels.cu) ----
+
+// classify + plan + scatter; d_state must be zeroed first. Returns launches.
+int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_state, uint8_t* d_cfg_of_cand,
+                     uint32_t* d_ids, cudaStream_t s, int num_sms, cudaError_t* err);
+
+// One plain launch of variant v. With d_state == nullptr the candidates are
+// indices [first, first+count) (no bucketing); otherwise shape `cfg`'s range
+// of the sorted id array, read from d_state on the device.
+cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
+                         int cfg, uint32_t first, uint32_t count, cudaStream_t s, int num_sms);
+
+// The persistent batched launch over the plan's first num_batched shapes.
+cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,
+                           BucketState* d_state, cudaStream_t s, int num_sms);
+
+// Bytes of shared memory one warp needs for a shape.
+uint32_t warp_smem_bytes(int v, int L);
+
+// Integer-ALU peak probe: `iters` rounds of independent 3-input logic ops.
+cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iters, cudaStream_t s);
+
+}  // namespace myers

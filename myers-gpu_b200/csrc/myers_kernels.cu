@@ -1,0 +1,605 @@
+// Myers bit-parallel candidate verification kernels for sm_100a.
+//
+// One candidate = one query (m bases, as PEQ bitmaps) against one window of
+// the 4-bit packed reference; the result is the first column of minimum
+// semi-global edit distance and that distance (the reference computes the
+// same in src-api/coreMyersGPU-CC50.cu:110-240 and, on the CPU,
+// src-integration/myers-reorderBuffer-padding.c:97-176).
+//
+// Layout of the work:
+//  * A candidate's query is a vector of 32*L*W rows held by L lanes, W
+//    32-bit words per lane. The query occupies the TOP m rows; the bottom
+//    p = 32*L*W - m rows are padding rows that match no base. Padding rows
+//    add exactly p to every score of the last row (row p of the DP is the
+//    constant p), so the score bit is always bit 31 of the top word and the
+//    argmin is unchanged; p is subtracted at the end.
+//  * Single-lane shapes (L = 1, W = 1..32): one candidate per lane, no lane
+//    exchange at all; the W-word add is one add.cc/addc chain.
+//  * Multi-lane shapes (L = 2..32): lane l holds rows [32*W*l, 32*W*(l+1)).
+//    Lanes run as a systolic pipeline: at step t lane l processes column
+//    t - l, taking the horizontal delta of its bottom row from lane l-1
+//    (that lane's top-row Ph/Mh bits of the same column, produced one step
+//    earlier) through __shfl_up_sync, with Myers' block rule (Eq |= hin<0,
+//    hin shifted into Ph/Mh). One shuffle pair per step; no carry ripple.
+//  * The PEQ of each candidate is staged once in shared memory, re-laid so
+//    that the W words a lane needs for one base are contiguous 16-byte
+//    groups (one LDS.128 per 4 words per column), already shifted to the
+//    top-aligned row layout.
+//  * The text is streamed per lane with one 32-bit load per 8 columns,
+//    prefetched one block ahead; a funnel shift realigns it for the exact
+//    window mode and for the per-lane skew of the systolic pipeline.
+//  * min(score, column) is tracked as one 32-bit key (score << 16 | column):
+//    an unsigned min keeps the smallest score and, among equal scores, the
+//    first column -- the reference's strict-< tie-break.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <utility>
+
+#include "myers_internal.h"
+
+namespace myers {
+
+#define FULL_MASK 0xFFFFFFFFu
+
+__device__ __forceinline__ uint32_t d_window_bases(uint32_t m, float distance) {
+  // (uint32_t)(m * (1 + 2*distance)) in float32, no contraction.
+  float f = __fadd_rn(1.0f, __fmul_rn(2.0f, distance));
+  return (uint32_t)__fmul_rn((float)m, f);
+}
+
+__device__ __forceinline__ uint32_t d_window_words(uint32_t wb) { return wb / 8 + ((wb % 8) ? 2u : 1u); }
+
+// Reference codes 5..7 behave as A (code 0) and bit 3 is ignored, as in the
+// reference kernel's select (src-api/coreMyersGPU-CC50.cu:82-95, :170).
+__device__ __forceinline__ uint32_t sanitize_codes(uint32_t t) {
+  uint32_t c = t & 0x77777777u;
+  uint32_t bad = (c + 0x33333333u) & 0x88888888u;  // nibbles holding 5..7
+  uint32_t mask = bad - (bad >> 3);                 // 0x7 in those nibbles
+  return c & ~mask;
+}
+
+__device__ __forceinline__ uint32_t ref_load(const uint32_t* __restrict__ ref, long long idx,
+                                             unsigned long long nwords) {
+  return (idx >= 0 && (unsigned long long)idx < nwords) ? __ldg(ref + idx) : kPadWord;
+}
+
+// Word x of the query's bit vector for base c (0 outside the query).
+__device__ __forceinline__ uint32_t qword(const uint32_t* __restrict__ peq, uint32_t pos_entry,
+                                          int nw, int c, int x) {
+  return (x >= 0 && x < nw) ? __ldg(peq + (size_t)(pos_entry + (uint32_t)(x >> 2)) * 20u + c * 4 + (x & 3))
+                            : 0u;
+}
+
+// Stage lane l's W words (of a 32*LW-row top-aligned query) for all five
+// bases: GW groups of [5 bases][4 words].
+template <int W>
+__device__ __forceinline__ void stage_lane(uint32_t* __restrict__ dst, const uint32_t* __restrict__ peq,
+                                           uint32_t pos_entry, uint32_t m, int LW, int l) {
+  constexpr int GW = (W + 3) / 4;
+  const int nw = (int)((m + 31) >> 5);
+  const int p = LW * 32 - (int)m;
+  const int pw = p >> 5, ps = p & 31;
+#pragma unroll 1
+  for (int g = 0; g < GW; ++g) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      uint32_t v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int a = l * W + 4 * g + j - pw;
+        uint32_t hi = qword(peq, pos_entry, nw, c, a);
+        uint32_t lo = qword(peq, pos_entry, nw, c, a - 1);
+        v[j] = ps ? __funnelshift_r(lo, hi, 32 - ps) : hi;
+      }
+      *reinterpret_cast<uint4*>(dst + (g * 5 + c) * 4) = make_uint4(v[0], v[1], v[2], v[3]);
+    }
+  }
+}
+
+// The W Eq words of one base; `p` points at the base's row of group 0.
+template <int W>
+__device__ __forceinline__ void load_eq(const uint32_t* __restrict__ p, uint32_t (&eq)[W]) {
+#pragma unroll
+  for (int g = 0; g < (W + 3) / 4; ++g) {
+    const uint32_t* q = p + g * 20;
+    if (4 * g + 4 <= W) {
+      uint4 v = *reinterpret_cast<const uint4*>(q);
+      eq[4 * g] = v.x;
+      eq[4 * g + 1] = v.y;
+      eq[4 * g + 2] = v.z;
+      eq[4 * g + 3] = v.w;
+    } else if (W - 4 * g >= 2) {
+      uint2 v = *reinterpret_cast<const uint2*>(q);
+      eq[4 * g] = v.x;
+      eq[4 * g + 1] = v.y;
+      if (W - 4 * g == 3) eq[4 * g + 2] = q[2];
+    } else {
+      eq[4 * g] = q[0];
+    }
+  }
+}
+
+// s = a + b over W words with the carry rippling through the CC flag.
+template <int W>
+__device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t (&b)[W], uint32_t (&s)[W]) {
+  if constexpr (W == 1) {
+    s[0] = a[0] + b[0];
+  } else {
+    asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(a[0]), "r"(b[0]));
+#pragma unroll
+    for (int j = 1; j < W - 1; ++j)
+      asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s[j]) : "r"(a[j]), "r"(b[j]));
+    asm volatile("addc.u32 %0, %1, %2;" : "=r"(s[W - 1]) : "r"(a[W - 1]), "r"(b[W - 1]));
+  }
+}
+
+// One text column over W words. With HIN, bit 31 of inP / inM is the
+// horizontal delta (+1 / -1) entering the bottom row (Myers' block rule);
+// without, it is 0 (semi-global: row 0 of the DP is all zeros).
+// topP / topM return the unshifted top words (bit 31 = delta out of the top row).
+template <int W, bool HIN>
+__device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (&Pv)[W], uint32_t (&Mv)[W],
+                                             uint32_t inP, uint32_t inM, uint32_t& topP, uint32_t& topM) {
+  uint32_t e0 = eq[0];
+  if (HIN) e0 |= inM >> 31;
+  uint32_t t[W], s[W];
+  t[0] = e0 & Pv[0];
+#pragma unroll
+  for (int j = 1; j < W; ++j) t[j] = eq[j] & Pv[j];
+  add_chain<W>(t, Pv, s);
+  uint32_t php = HIN ? inP : 0u, mhp = HIN ? inM : 0u;
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    const uint32_t e = (j == 0) ? e0 : eq[j];
+    const uint32_t pv = Pv[j], mv = Mv[j];
+    const uint32_t xv = eq[j] | mv;
+    const uint32_t xh = (s[j] ^ pv) | e;
+    const uint32_t ph = mv | ~(xh | pv);
+    const uint32_t mh = pv & xh;
+    const uint32_t phs = __funnelshift_l(php, ph, 1);
+    const uint32_t mhs = __funnelshift_l(mhp, mh, 1);
+    Pv[j] = mhs | ~(xv | phs);
+    Mv[j] = phs & xv;
+    php = ph;
+    mhp = mh;
+  }
+  topP = php;
+  topM = mhp;
+}
+
+// Eight columns of one text word, single-lane shapes. TAIL masks columns >= n.
+template <int W, bool TAIL>
+__device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
+                                              uint32_t (&Mv)[W], uint32_t& sc, uint32_t& kmin,
+                                              uint32_t colbase, uint32_t n) {
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const uint32_t off = ((t >> (4 * u)) & 7u) << 4;
+    uint32_t eq[W];
+    load_eq<W>(reinterpret_cast<const uint32_t*>(slot + off), eq);
+    uint32_t tp, tm;
+    myers_column<W, false>(eq, Pv, Mv, 0u, 0u, tp, tm);
+    sc += (tp >> 31) << 16;
+    sc -= (tm >> 31) << 16;
+    const uint32_t key = sc + colbase + (uint32_t)u;
+    if (!TAIL || colbase + (uint32_t)u < n) kmin = min(kmin, key);
+  }
+}
+
+struct CandSetup {
+  uint32_t id;
+  unsigned long long pos;
+  uint32_t m;
+  uint32_t pos_entry;
+  uint32_t n;     // columns
+  bool has;       // the slot holds a candidate
+  bool work;      // ... that needs the DP
+};
+
+// Checks that keep every device read of a candidate inside its buffers.
+// Returns 0 if the candidate can be verified, else the flag to raise.
+__device__ __forceinline__ uint32_t check_query(const DevInputs& in, uint32_t query, uint2 q) {
+  if (query >= in.num_queries) return kFlagBadQuery;
+  if ((unsigned long long)q.x + ((q.y + 127u) >> 7) > in.num_entries) return kFlagBadEntry;
+  return 0u;
+}
+
+// Resolve the candidate of this segment and write the result of candidates
+// that need no DP (window out of range, empty query, unsupported size,
+// invalid indices).
+__device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const uint32_t* __restrict__ ids,
+                                                     uint32_t first, uint32_t cnt, int seg, int nseg,
+                                                     int l, int rows) {
+  CandSetup c;
+  c.has = seg < nseg && (uint32_t)seg < cnt;
+  c.id = 0;
+  c.pos = 0;
+  c.m = 0;
+  c.pos_entry = 0;
+  c.n = 0;
+  c.work = false;
+  if (c.has) {
+    c.id = ids ? __ldg(ids + first + seg) : first + (uint32_t)seg;
+    const Cand cd = in.cands[c.id];
+    uint2 q = make_uint2(0u, 0u);
+    uint32_t bad = 0u;
+    if (cd.query < in.num_queries) q = __ldg(in.qinfo + cd.query);
+    bad = check_query(in, cd.query, q);
+    c.pos = cd.position;
+    c.pos_entry = q.x;
+    c.m = q.y;
+    const uint32_t wb = d_window_bases(c.m, in.distance);
+    const bool valid = bad == 0u && c.pos < in.ref_size && (in.ref_size - c.pos) > (unsigned long long)wb;
+    c.n = in.exact ? wb : 8u * d_window_words(wb);
+    const bool fits = c.m <= (uint32_t)rows && c.n <= kMaxColumns;
+    c.work = valid && c.m > 0 && fits;
+    if (!c.work && l == 0) {
+      in.results[c.id] = (valid && c.m == 0) ? make_uint2(0u, 0u) : make_uint2(0u, kNoResult);
+      if (bad) atomicOr(in.flags, bad);
+      else if (valid && c.m > 0 && !fits) atomicOr(in.flags, kFlagUnsupported);
+    }
+  }
+  return c;
+}
+
+template <int W, bool MULTI>
+__device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
+                                             uint32_t cnt, int L, uint32_t* __restrict__ wsmem, int lane) {
+  constexpr int GW = (W + 3) / 4;
+  const int Lr = MULTI ? L : 1;
+  const int nseg = MULTI ? 32 / L : 32;
+  const int seg = MULTI ? lane / L : lane;
+  const int l = MULTI ? lane - seg * L : 0;
+  const int LW = Lr * W;
+  const int rows = 32 * LW;
+  // lanes past the last segment (L not dividing 32) read segment 0's slot
+  const int sseg = seg < nseg ? seg : 0;
+  uint32_t* lane_part = wsmem + (sseg * Lr + l) * GW * 20;
+
+  const CandSetup c = setup_candidate(in, ids, first, cnt, seg, nseg, l, rows);
+  if (c.work) stage_lane<W>(lane_part, in.peq, c.pos_entry, c.m, LW, l);
+  __syncwarp();
+
+  const uint32_t p = (uint32_t)rows - c.m;
+  uint32_t Pv[W], Mv[W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    Pv[j] = 0xFFFFFFFFu;
+    Mv[j] = 0u;
+  }
+  uint32_t sc = (uint32_t)rows << 16;  // score + p = rows at column -1
+  uint32_t kmin = sc;                  // (score, column) = (m, 0) before any column
+  const long long q0 = (long long)(in.exact ? c.pos : (c.pos & ~7ull)) - l;
+  const long long b0 = q0 >> 3;
+  const uint32_t sh = 4u * (uint32_t)(q0 & 7);
+  const char* slot = reinterpret_cast<const char*>(lane_part);
+
+  if constexpr (!MULTI) {
+    if (c.work) {
+      uint32_t lo = ref_load(in.ref, b0, in.ref_words);
+      uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
+      const uint32_t nfull = c.n >> 3;
+      uint32_t i = 0;
+      for (; i < nfull; ++i) {
+        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+        lo = hi;
+        hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+        block8_single<W, false>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n);
+      }
+      if (c.n & 7u) {
+        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+        block8_single<W, true>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n);
+      }
+      in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
+    }
+  } else {
+    uint32_t steps = c.work ? c.n + (uint32_t)L - 1u : 0u;
+    steps = __reduce_max_sync(FULL_MASK, steps);
+    const uint32_t nblk = (steps + 7u) >> 3;
+    uint32_t lo = ref_load(in.ref, b0, in.ref_words);
+    uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
+    uint32_t outP = 0u, outM = 0u;
+    const bool seg_start = (l == 0);
+    for (uint32_t i = 0; i < nblk; ++i) {
+      const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+      lo = hi;
+      hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const uint32_t off = ((t >> (4 * u)) & 7u) << 4;
+        uint32_t eq[W];
+        load_eq<W>(reinterpret_cast<const uint32_t*>(slot + off), eq);
+        uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1);
+        uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1);
+        if (seg_start) {
+          inP = 0u;
+          inM = 0u;
+        }
+        const uint32_t j = 8u * i + (uint32_t)u - (uint32_t)l;  // wraps when negative
+        if (c.work && j < c.n) {
+          myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM);
+          sc += (outP >> 31) << 16;
+          sc -= (outM >> 31) << 16;
+          kmin = min(kmin, sc + j);
+        }
+      }
+    }
+    if (c.work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
+  }
+  __syncwarp();
+}
+
+template <int W, bool MULTI>
+__host__ __device__ constexpr uint32_t warp_words(int L) {
+  return (uint32_t)((MULTI ? (32 / L) * L : 32) * ((W + 3) / 4) * 20);
+}
+
+// Plain launch: one shape over a contiguous range of (sorted) candidates,
+// grid-stride over warp tiles.
+template <int W, bool MULTI>
+__global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __restrict__ ids,
+                                               const BucketState* __restrict__ st, int cfg, uint32_t first,
+                                               uint32_t count, int L) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (st != nullptr) {
+    first = st->first[cfg];
+    count = st->count[cfg];
+  }
+  const int nseg = MULTI ? 32 / L : 32;
+  uint32_t* wsmem = smem + wib * warp_words<W, MULTI>(L);
+  const uint32_t tiles = (count + nseg - 1) / nseg;
+  const uint32_t wpb = blockDim.x >> 5;
+  for (uint32_t t = blockIdx.x * wpb + wib; t < tiles; t += gridDim.x * wpb) {
+    const uint32_t f = t * nseg;
+    const uint32_t cnt = min((uint32_t)nseg, count - f);
+    process_tile<W, MULTI>(in, ids, first + f, cnt, L, wsmem, lane);
+  }
+}
+
+// ---- length bucketing on the device ----
+
+__global__ void k_classify(DevInputs in, const __grid_constant__ PlanTable plan, BucketState* st,
+                           uint8_t* __restrict__ cfg_of_cand) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t n = in.num_cands;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += stride) {
+    const uint32_t i = base + lane;
+    uint32_t cfg = kNoCfg;
+    if (i < n) {
+      const Cand cd = in.cands[i];
+      uint2 q = make_uint2(0u, 0u);
+      if (cd.query < in.num_queries) q = __ldg(in.qinfo + cd.query);
+      const uint32_t bad = check_query(in, cd.query, q);
+      const uint32_t m = q.y;
+      const uint32_t wb = d_window_bases(m, in.distance);
+      const bool valid = bad == 0u && cd.position < in.ref_size &&
+                         (in.ref_size - cd.position) > (unsigned long long)wb;
+      const uint32_t ncol = in.exact ? wb : 8u * d_window_words(wb);
+      if (bad) {
+        in.results[i] = make_uint2(0u, kNoResult);
+        atomicOr(in.flags, bad);
+      } else if (!valid) {
+        in.results[i] = make_uint2(0u, kNoResult);
+      } else if (m == 0) {
+        in.results[i] = make_uint2(0u, 0u);
+      } else if (m > kMaxWords * 32 || ncol > kMaxColumns || plan.cfg_of_words[(m + 31) >> 5] == kNoCfg) {
+        in.results[i] = make_uint2(0u, kNoResult);
+        atomicOr(in.flags, kFlagUnsupported);
+      } else {
+        cfg = plan.cfg_of_words[(m + 31) >> 5];
+      }
+      cfg_of_cand[i] = (uint8_t)cfg;
+    }
+    const unsigned peers = __match_any_sync(FULL_MASK, cfg);
+    if (cfg != kNoCfg && lane == __ffs(peers) - 1) atomicAdd(&st->count[cfg], (uint32_t)__popc(peers));
+  }
+}
+
+__global__ void k_plan(const __grid_constant__ PlanTable plan, BucketState* st) {
+  if (threadIdx.x != 0) return;
+  uint32_t acc = 0, tiles = 0;
+  for (uint32_t c = 0; c < plan.num_cfg; ++c) {
+    const Shape s = plan.shape[c];
+    const uint32_t nseg = (s.variant >= kNumSingle) ? 32u / s.L : 32u;
+    if (c == plan.num_batched) st->total_tiles = tiles;
+    st->first[c] = acc;
+    st->cursor[c] = 0;
+    st->tile_start[c] = tiles;
+    tiles += (st->count[c] + nseg - 1) / nseg;
+    acc += st->count[c];
+  }
+  st->tile_start[plan.num_cfg] = tiles;
+  if (plan.num_batched >= plan.num_cfg) st->total_tiles = tiles;
+  st->queue = 0;
+}
+
+// Stable within each warp's 32 consecutive candidates, so the candidates of
+// one read (adjacent in the input) mostly stay adjacent.
+__global__ void k_scatter(uint32_t n, const uint8_t* __restrict__ cfg_of_cand, BucketState* st,
+                          uint32_t* __restrict__ ids) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += stride) {
+    const uint32_t i = base + lane;
+    const uint32_t cfg = i < n ? cfg_of_cand[i] : kNoCfg;
+    const unsigned peers = __match_any_sync(FULL_MASK, cfg);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t b = 0;
+    if (cfg != kNoCfg && lane == leader) b = atomicAdd(&st->cursor[cfg], (uint32_t)__popc(peers));
+    b = __shfl_sync(FULL_MASK, b, leader);
+    if (cfg != kNoCfg) ids[st->first[cfg] + b + rank] = i;
+  }
+}
+
+// ---- the persistent batched kernel ----
+
+constexpr uint32_t kBatchedWarpWords = 32 * ((kBatchedMaxW + 3) / 4) * 20;  // the largest batched shape
+
+template <int V>
+__device__ __forceinline__ void dispatch_one(const DevInputs& in, const uint32_t* ids, uint32_t f, uint32_t cnt,
+                                             int L, uint32_t* wsmem, int lane) {
+  if constexpr (V < kNumSingle) {
+    if constexpr (V + 1 <= kBatchedMaxW) process_tile<V + 1, false>(in, ids, f, cnt, L, wsmem, lane);
+  } else {
+    if constexpr (kMultiW[V - kNumSingle] <= kBatchedMaxW)
+      process_tile<kMultiW[V - kNumSingle], true>(in, ids, f, cnt, L, wsmem, lane);
+  }
+}
+
+template <int... Vs>
+__device__ __forceinline__ void dispatch(int v, const DevInputs& in, const uint32_t* ids, uint32_t f, uint32_t cnt,
+                                         int L, uint32_t* wsmem, int lane, std::integer_sequence<int, Vs...>) {
+  ((v == Vs ? (dispatch_one<Vs>(in, ids, f, cnt, L, wsmem, lane), 0) : 0), ...);
+}
+
+// Each warp pulls the next tile index from the device queue; tiles are
+// ordered by shape, most expensive shape first, so the long candidates start
+// early and the short ones fill the tail.
+__global__ void __launch_bounds__(128) k_batched(DevInputs in, const uint32_t* __restrict__ ids,
+                                                 const __grid_constant__ PlanTable plan, BucketState* st) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t s_tile_start[kMaxCfg + 1];
+  __shared__ uint32_t s_first[kMaxCfg];
+  __shared__ uint32_t s_count[kMaxCfg];
+  __shared__ Shape s_shape[kMaxCfg];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t ncfg = plan.num_batched;
+  for (uint32_t c = threadIdx.x; c < ncfg; c += blockDim.x) {
+    s_tile_start[c] = st->tile_start[c];
+    s_first[c] = st->first[c];
+    s_count[c] = st->count[c];
+    s_shape[c] = plan.shape[c];
+  }
+  __syncthreads();
+  const uint32_t total = st->total_tiles;
+  uint32_t* wsmem = smem + wib * kBatchedWarpWords;
+  while (true) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(&st->queue, 1u);
+    t = __shfl_sync(FULL_MASK, t, 0);
+    if (t >= total) break;
+    // last shape whose first tile is <= t
+    uint32_t lo = 0, hi = ncfg - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (s_tile_start[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const Shape s = s_shape[lo];
+    const int L = s.L;
+    const uint32_t nseg = (s.variant >= kNumSingle) ? 32u / (uint32_t)L : 32u;
+    const uint32_t f = (t - s_tile_start[lo]) * nseg;
+    const uint32_t cnt = min(nseg, s_count[lo] - f);
+    dispatch(s.variant, in, ids, s_first[lo] + f, cnt, L, wsmem, lane,
+             std::make_integer_sequence<int, kNumVariants>{});
+  }
+}
+
+// Integer-ALU peak probe: eight independent chains of 3-input logic ops per
+// thread (the instruction class of the Myers column), written out so the
+// work cannot be removed.
+__global__ void k_lop3_probe(uint32_t* out, int iters) {
+  uint32_t a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = threadIdx.x * (k + 3) + blockIdx.x;
+  uint32_t b = threadIdx.x ^ 0x5A5A5A5Au;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(a[k]) : "r"(a[(k + 1) & 7]), "r"(b));
+    }
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x ^= a[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = x;
+}
+
+// ---- host-side launchers ----
+
+using PlainFn = void (*)(DevInputs, const uint32_t*, const BucketState*, int, uint32_t, uint32_t, int);
+
+template <int V>
+constexpr PlainFn plain_fn() {
+  if constexpr (V < kNumSingle) return &k_plain<V + 1, false>;
+  else return &k_plain<kMultiW[V - kNumSingle], true>;
+}
+
+template <int... Vs>
+constexpr auto make_plain_table(std::integer_sequence<int, Vs...>) {
+  struct T { PlainFn f[sizeof...(Vs)]; };
+  return T{{plain_fn<Vs>()...}};
+}
+
+static const auto kPlainTable = make_plain_table(std::make_integer_sequence<int, kNumVariants>{});
+
+uint32_t warp_smem_bytes(int v, int L) {
+  const int W = variant_W(v);
+  const int gw = (W + 3) / 4;
+  const int lanes = variant_multi(v) ? (32 / L) * L : 32;
+  return (uint32_t)(lanes * gw * 20 * 4);
+}
+
+static int blocks_per_sm(const void* fn, int threads, size_t smem) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess || nb < 1) nb = 1;
+  return nb;
+}
+
+cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
+                         int cfg, uint32_t first, uint32_t count, cudaStream_t s, int num_sms) {
+  const PlainFn fn = kPlainTable.f[v];
+  const int threads = 128;
+  const int Lr = variant_multi(v) ? L : 1;
+  const size_t smem = (size_t)warp_smem_bytes(v, Lr) * (threads / 32);
+  cudaError_t e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int nb = blocks_per_sm((const void*)fn, threads, smem);
+  uint32_t grid = (uint32_t)(num_sms * nb);
+  if (d_state == nullptr) {
+    const uint32_t nseg = variant_multi(v) ? 32u / (uint32_t)L : 32u;
+    const uint32_t tiles = (count + nseg - 1) / nseg;
+    const uint32_t need = (tiles + threads / 32 - 1) / (threads / 32);
+    if (need < grid) grid = need;
+    if (grid == 0) return cudaSuccess;
+  }
+  fn<<<grid, threads, smem, s>>>(in, d_ids, d_state, cfg, first, count, Lr);
+  return cudaGetLastError();
+}
+
+int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_state, uint8_t* d_cfg_of_cand,
+                     uint32_t* d_ids, cudaStream_t s, int num_sms, cudaError_t* err) {
+  const int threads = 256;
+  const uint32_t need = (in.num_cands + threads - 1) / threads;
+  uint32_t grid = (uint32_t)num_sms * 8;
+  if (need < grid) grid = need > 0 ? need : 1;
+  k_classify<<<grid, threads, 0, s>>>(in, plan, d_state, d_cfg_of_cand);
+  k_plan<<<1, 32, 0, s>>>(plan, d_state);
+  k_scatter<<<grid, threads, 0, s>>>(in.num_cands, d_cfg_of_cand, d_state, d_ids);
+  *err = cudaGetLastError();
+  return 3;
+}
+
+cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,
+                           BucketState* d_state, cudaStream_t s, int num_sms) {
+  const int threads = 128;
+  const size_t smem = (size_t)kBatchedWarpWords * 4 * (threads / 32);
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const int nb = blocks_per_sm((const void*)k_batched, threads, smem);
+  k_batched<<<num_sms * nb, threads, smem, s>>>(in, d_ids, plan, d_state);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iters, cudaStream_t s) {
+  k_lop3_probe<<<blocks, threads, 0, s>>>(d_out, iters);
+  return cudaGetLastError();
+}
+
+}  // namespace myers

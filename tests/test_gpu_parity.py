@@ -1,0 +1,234 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the oracle
+(the reference's own CPU Myers via golden vectors, and the restated oracle on
+seeded workloads). Integer outputs: bit-exact."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DIST = 0.2
+
+
+@pytest.fixture(scope="module")
+def gpu(mg, cuda_ok):
+    import torch
+    torch.cuda.init()
+    return mg
+
+
+def _run(mg, ref_words, ref_size, peq, qinfo, cands, window, path, distance=DIST, min_size=0, max_size=0):
+    ref = mg.Reference(ref_words, ref_size)
+    ctx = mg.Context(max(1, len(cands)))
+    try:
+        res = mg.verify_torch(ctx, ref, peq, qinfo, cands, distance, window=window, path=path, min_size=min_size,
+                              max_size=max_size)
+        return res, ctx.launches(), ctx.flags()
+    finally:
+        ctx.close()
+        ref.close()
+
+
+@pytest.mark.parametrize("path", ["plain", "batched"])
+def test_golden_aligned(gpu, golden_verify, path):
+    g = golden_verify
+    p = gpu.PATH_PLAIN if path == "plain" else gpu.PATH_BATCHED
+    res, launches, flags = _run(gpu, g["ref"], g["ref_size"], g["peq"], g["qinfo"], g["cands"], gpu.WINDOW_ALIGNED, p,
+                                distance=g["distance"])
+    bad = np.nonzero(res != g["res_aligned"])[0]
+    assert bad.size == 0, (bad[:10], res[bad[:10]], g["res_aligned"][bad[:10]])
+    assert launches >= 1 and flags == 0
+
+
+@pytest.mark.parametrize("path", ["plain", "batched"])
+def test_golden_exact(gpu, golden_verify, path):
+    g = golden_verify
+    p = gpu.PATH_PLAIN if path == "plain" else gpu.PATH_BATCHED
+    m = g["exact_mask"]
+    res, _, _ = _run(gpu, g["ref"], g["ref_size"], g["peq"], g["qinfo"], g["cands"], gpu.WINDOW_EXACT, p,
+                     distance=g["distance"])
+    assert np.array_equal(res[m], g["res_exact"][m])
+
+
+WORKLOADS = [(1, 0.05), (2, 0.004), (3, 0.002), (4, 0.003), (5, 0.004)]
+
+
+@pytest.fixture(scope="module")
+def workloads(gpu):
+    ref_size = 8_000_000
+    ref = gpu.make_reference(ref_size, 1234)
+    out = {}
+    for k, scale in WORKLOADS:
+        out[k] = gpu.make_workload(gpu.workload_spec(k, scale=scale, ref_size=ref_size), ref)
+    return ref, ref_size, out
+
+
+@pytest.mark.parametrize("k", [k for k, _ in WORKLOADS])
+@pytest.mark.parametrize("window", ["aligned", "exact"])
+@pytest.mark.parametrize("path", ["plain", "batched"])
+def test_workloads_vs_oracle(gpu, orc, workloads, k, window, path):
+    ref, ref_size, ws = workloads
+    w = ws[k]
+    exact = window == "exact"
+    expect = orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST, exact=exact)
+    p = gpu.PATH_PLAIN if path == "plain" else gpu.PATH_BATCHED
+    res, launches, flags = _run(gpu, ref, ref_size, w["peq"], w["qinfo"], w["cands"],
+                                gpu.WINDOW_EXACT if exact else gpu.WINDOW_ALIGNED, p)
+    bad = np.nonzero(res != expect)[0]
+    assert bad.size == 0, (len(bad), bad[:5], res[bad[:5]], expect[bad[:5]])
+    assert flags == 0
+
+
+def test_uniform_length_single_launch(gpu, orc, workloads):
+    ref, ref_size, ws = workloads
+    w = ws[1]
+    res, launches, _ = _run(gpu, ref, ref_size, w["peq"], w["qinfo"], w["cands"], gpu.WINDOW_ALIGNED,
+                            gpu.PATH_PLAIN, min_size=100, max_size=100)
+    assert launches == 1
+    assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST))
+
+
+@pytest.mark.parametrize("variant_L", [(4, 2), (4, 9), (6, 6), (8, 4), (10, 3), (12, 3), (16, 2), (32, 2)])
+def test_every_multi_shape(gpu, orc, workloads, variant_L):
+    """Force each multi-lane variant (including L not dividing 32) on reads
+    of up to 1000 bases and compare with the oracle."""
+    W, L = variant_L
+    ref, ref_size, ws = workloads
+    w = ws[3]
+    v = [x for x, ww, multi in gpu.variants() if multi and ww == W][0]
+    words = sorted(set(((w["lengths"] + 31) // 32).tolist()))
+    try:
+        for wd in words:
+            if W * L >= wd:
+                gpu.set_shape_override(gpu.PATH_PLAIN, wd, v, L)
+        res, _, _ = _run(gpu, ref, ref_size, w["peq"], w["qinfo"], w["cands"], gpu.WINDOW_ALIGNED, gpu.PATH_PLAIN)
+    finally:
+        for wd in words:
+            gpu.set_shape_override(gpu.PATH_PLAIN, wd, -1)
+    assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST))
+
+
+def test_all_lengths_1_to_300(gpu, orc):
+    """Every query length 1..300 (every single-lane W up to 10 and every
+    top-alignment shift), both windows."""
+    rng = np.random.default_rng(7)
+    ref_size = 200_000
+    ref = gpu.make_reference(ref_size, 77)
+    peq, qinfo, cands = [], [], []
+    entry = 0
+    for q, m in enumerate(range(1, 301)):
+        read = bytes(rng.choice(list(b"ACGTN"), size=m, p=[0.245, 0.245, 0.245, 0.245, 0.02]).astype(np.uint8))
+        peq.append(orc.pack_peq(read).reshape(-1, 20))
+        qinfo.append((entry, m))
+        entry += (m + 127) // 128
+        for _ in range(4):
+            cands.append((q, int(rng.integers(0, ref_size - 500))))
+    peq = np.concatenate(peq).ravel().view(gpu.QRY_ENTRY)
+    qinfo = np.array(qinfo, dtype=np.uint32).view(gpu.QINFO).ravel()
+    c = np.zeros(len(cands), dtype=gpu.CAND)
+    c["query"] = [x[0] for x in cands]
+    c["position"] = [x[1] for x in cands]
+    for exact in (False, True):
+        expect = orc.verify(peq, qinfo, c, ref, ref_size, DIST, exact=exact)
+        for path in (gpu.PATH_PLAIN, gpu.PATH_BATCHED):
+            res, _, _ = _run(gpu, ref, ref_size, peq, qinfo, c, gpu.WINDOW_EXACT if exact else gpu.WINDOW_ALIGNED,
+                             path)
+            assert np.array_equal(res, expect)
+
+
+def test_long_queries_up_to_max(gpu, orc):
+    """Queries at the multi-lane limits (16384 batched, 32768 plain)."""
+    rng = np.random.default_rng(3)
+    ref_size = 400_000
+    ref = gpu.make_reference(ref_size, 5)
+    peq, qinfo, cands = [], [], []
+    entry = 0
+    for q, m in enumerate([4097, 10000, 16384, 20000, 32768]):
+        start = int(rng.integers(0, ref_size - 2 * m))
+        codes = [(int(ref[(start + k) // 8]) >> (4 * ((start + k) % 8))) & 0xF for k in range(m)]
+        read = bytes(b"ACGTN"[c] if rng.random() > 0.05 else b"ACGT"[rng.integers(0, 4)] for c in codes)
+        peq.append(orc.pack_peq(read).reshape(-1, 20))
+        qinfo.append((entry, m))
+        entry += (m + 127) // 128
+        cands.append((q, max(0, start - m // 5)))
+        cands.append((q, int(rng.integers(0, ref_size - 2 * m))))
+    peq = np.concatenate(peq).ravel().view(gpu.QRY_ENTRY)
+    qinfo = np.array(qinfo, dtype=np.uint32).view(gpu.QINFO).ravel()
+    c = np.zeros(len(cands), dtype=gpu.CAND)
+    c["query"] = [x[0] for x in cands]
+    c["position"] = [x[1] for x in cands]
+    expect = orc.verify(peq, qinfo, c, ref, ref_size, DIST)
+    for path in (gpu.PATH_PLAIN, gpu.PATH_BATCHED):
+        res, _, flags = _run(gpu, ref, ref_size, peq, qinfo, c, gpu.WINDOW_ALIGNED, path)
+        assert np.array_equal(res, expect)
+        assert flags == 0
+
+
+def test_invalid_indices_are_flagged(gpu, orc):
+    """Bad query indices and PEQ entries give {0, MAX} and a flag, never a
+    wild read; the valid candidates around them are unaffected."""
+    ref_size = 100_000
+    ref = gpu.make_reference(ref_size, 8)
+    w = gpu.make_workload(gpu.workload_spec(1, scale=0.001, ref_size=ref_size), ref)
+    cands = w["cands"].copy()
+    qinfo = w["qinfo"].copy()
+    cands[3]["query"] = len(qinfo) + 10           # query out of range
+    qinfo[5]["posEntry"] = len(w["peq"]) + 100     # PEQ entries out of range
+    expect = orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST)
+    for path in (gpu.PATH_PLAIN, gpu.PATH_BATCHED):
+        res, _, flags = _run(gpu, ref, ref_size, w["peq"], qinfo, cands, gpu.WINDOW_ALIGNED, path)
+        assert res[3]["score"] == gpu.NO_RESULT
+        bad5 = cands["query"] == 5
+        assert (res[bad5]["score"] == gpu.NO_RESULT).all()
+        ok = (cands["query"] != 5) & (np.arange(len(cands)) != 3)
+        assert np.array_equal(res[ok], expect[ok])
+        assert flags & 2 and flags & 4
+
+
+def test_empty_and_zero_length(gpu, orc):
+    ref_size = 10_000
+    ref = gpu.make_reference(ref_size, 2)
+    peq = np.zeros(1, dtype=gpu.QRY_ENTRY)
+    qinfo = np.array([(0, 0)], dtype=np.uint32).view(gpu.QINFO).ravel()
+    c = np.zeros(3, dtype=gpu.CAND)
+    c["position"] = [0, 5000, ref_size + 1]
+    for path in (gpu.PATH_PLAIN, gpu.PATH_BATCHED):
+        res, _, _ = _run(gpu, ref, ref_size, peq, qinfo, c, gpu.WINDOW_ALIGNED, path)
+        assert res.tolist() == orc.verify(peq, qinfo, c, ref, ref_size, DIST).tolist()
+        assert res.tolist() == [(0, 0), (0, 0), (0, gpu.NO_RESULT)]
+        res0, launches, _ = _run(gpu, ref, ref_size, peq, qinfo, c[:0], gpu.WINDOW_ALIGNED, path)
+        assert len(res0) == 0 and launches == 0
+
+
+def _write_ref_file(path, words, size):
+    with open(path, "wb") as f:
+        f.write(np.array([len(words), size], dtype=np.uint32).tobytes())
+        f.write(np.asarray(words, dtype=np.uint32).tobytes())
+
+
+@pytest.mark.parametrize("path", ["plain", "batched"])
+def test_dropin_buffers(gpu, orc, workloads, path):
+    """The reference's call sequence: initMyers, fill the pinned buffers
+    through the getters, send, receive, read results, endMyers."""
+    ref, ref_size, ws = workloads
+    with tempfile.TemporaryDirectory() as tmp:
+        fn = os.path.join(tmp, "g.4bits.ref")
+        _write_ref_file(fn, ref, ref_size)
+        gpu.lib.myersSetMemoryBudget(256 << 20)
+        bufs = gpu.Buffers(fn, num_buffers=2, avg_query_size=400, cands_per_query=10)
+        try:
+            bufs.set_path(gpu.PATH_PLAIN if path == "plain" else gpu.PATH_BATCHED)
+            for i, k in enumerate((3, 5)):
+                w = ws[k]
+                res, st = gpu.verify_buffers(bufs, w["peq"], w["qinfo"], w["cands"], DIST, buffer=i)
+                assert st == gpu.SUCCESS
+                assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST))
+            # capacity errors are returned, not fatal
+            ne, nq, nc = bufs.capacity(0)
+            st = gpu.lib.myersSend(bufs.handles[0], DIST, ne + 1, 1, 1)
+            assert st == gpu.E_CAPACITY
+        finally:
+            bufs.close()
+            gpu.lib.myersSetMemoryBudget(0)

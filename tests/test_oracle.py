@@ -1,0 +1,140 @@
+"""CPU tests: the oracle against the reference's golden vectors and a textbook
+DP, the packers against the reference's packers, the workload generator."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def test_oracle_matches_reference_aligned(golden_verify, orc):
+    g = golden_verify
+    res = orc.verify(g["peq"], g["qinfo"], g["cands"], g["ref"], g["ref_size"], g["distance"])
+    assert np.array_equal(res, g["res_aligned"].astype(res.dtype))
+
+
+def test_oracle_matches_reference_exact(golden_verify, orc):
+    g = golden_verify
+    m = g["exact_mask"]
+    res = orc.verify(g["peq"], g["qinfo"], g["cands"], g["ref"], g["ref_size"], g["distance"], exact=True)
+    assert np.array_equal(res[m], g["res_exact"][m].astype(res.dtype))
+
+
+def test_golden_covers_edges(golden_verify):
+    g = golden_verify
+    sizes = g["qinfo"]["size"]
+    pos = g["cands"]["position"]
+    assert set(np.unique(pos % 8)) == set(range(8))
+    for m in (1, 31, 32, 33, 127, 128, 129, 1024, 1025, 4096):
+        assert m in sizes
+    assert (g["res_aligned"]["score"] == 0xFFFFFFFF).sum() > 0          # out-of-range windows
+    assert sizes.max() > 4096                                            # beyond the API's old cap
+
+
+def _codes(ref_words, start, n):
+    return [(int(ref_words[(start + k) // 8]) >> (4 * ((start + k) % 8))) & 0xF for k in range(n)]
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_matches_textbook_dp(orc, mg, seed):
+    rng = np.random.default_rng(seed)
+    ref_size = 3000
+    ascii_ref = bytes(rng.choice(list(b"ACGTN"), size=ref_size, p=[0.24, 0.24, 0.24, 0.24, 0.04]).astype(np.uint8))
+    words = orc.pack_reference(ascii_ref)
+    peq, qinfo, cands, expect_a, expect_e = [], [], [], [], []
+    entry = 0
+    for q in range(12):
+        m = int(rng.integers(1, 80))
+        read = bytes(rng.choice(list(b"ACGTN"), size=m).astype(np.uint8))
+        peq.append(orc.pack_peq(read).reshape(-1, 20))
+        qinfo.append((entry, m))
+        entry += (m + 127) // 128
+        W = orc.window_bases(m, 0.2)
+        for _ in range(3):
+            pos = int(rng.integers(0, ref_size - W - 20))
+            cands.append((q, pos))
+            qc = ["ACGTN".index(chr(b)) for b in read]
+            E = W // 8 + (2 if W % 8 else 1)
+            start = pos - pos % 8
+            expect_a.append(orc.dp_semiglobal(qc, _codes(words, start, 8 * E)))
+            expect_e.append(orc.dp_semiglobal(qc, _codes(words, pos, W)))
+    peq = np.concatenate(peq).ravel().view(mg.QRY_ENTRY)
+    qinfo = np.array(qinfo, dtype=np.uint32).view(mg.QINFO).ravel()
+    c = np.zeros(len(cands), dtype=mg.CAND)
+    c["query"] = [x[0] for x in cands]
+    c["position"] = [x[1] for x in cands]
+    ra = orc.verify(peq, qinfo, c, words, ref_size, 0.2)
+    re_ = orc.verify(peq, qinfo, c, words, ref_size, 0.2, exact=True)
+    assert [(int(r["score"]), int(r["column"])) for r in ra] == expect_a
+    assert [(int(r["score"]), int(r["column"])) for r in re_] == expect_e
+
+
+def test_reference_packer_format(orc):
+    d = np.load(os.path.join(GOLDEN, "packers.npz"))
+    fasta = d["fasta"].tobytes()
+    seq = b"".join(line for line in fasta.split(b"\n") if line and not line.startswith(b">"))
+    ref_file = d["ref_file"].tobytes()
+    num_entries, size = np.frombuffer(ref_file[:8], dtype=np.uint32)
+    assert size == len(seq) and num_entries == (len(seq) + 7) // 8
+    ref_words = np.frombuffer(ref_file[8:], dtype=np.uint32)
+    mine = orc.pack_reference(seq)
+    full = size // 8  # the reference packs the partial last word from stale bytes
+    assert np.array_equal(mine[:full], ref_words[:full])
+    last_mask = (1 << (4 * (size % 8))) - 1
+    assert (int(mine[full]) & last_mask) == (int(ref_words[full]) & last_mask)
+
+
+def test_reference_peq_format(orc, mg):
+    d = np.load(os.path.join(GOLDEN, "packers.npz"))
+    prof = d["prof"].tobytes().strip().split(b"\n")
+    qry = d["qry_file"].tobytes()
+    hdr = np.frombuffer(qry[:20], dtype=np.uint32)
+    _, tot_entries, _, nq, nc = (int(x) for x in hdr)
+    off = 20
+    peq = np.frombuffer(qry[off:off + 80 * tot_entries], dtype=np.uint32).reshape(-1, 20)
+    off += 80 * tot_entries
+    cands = np.frombuffer(qry[off:off + 16 * nc], dtype=mg.CAND)
+    off += 16 * nc
+    qinfo = np.frombuffer(qry[off:off + 8 * nq], dtype=mg.QINFO)
+    assert nq == len(prof)
+    entry = 0
+    for i, line in enumerate(prof):
+        read = line.split(b"\t")[0]
+        assert qinfo[i]["size"] == len(read) and qinfo[i]["posEntry"] == entry
+        ne = (len(read) + 127) // 128
+        assert np.array_equal(orc.pack_peq(read).reshape(-1, 20), peq[entry:entry + ne])
+        entry += ne
+        for j, tok in enumerate(line.split(b"\t")[1:]):
+            assert cands[3 * i + j]["query"] == i
+            assert cands[3 * i + j]["position"] == int(tok.split(b":")[2])
+
+
+def test_synth_deterministic(mg):
+    r1 = mg.make_reference(1_000_000, 5)
+    r2 = mg.make_reference(1_000_000, 5)
+    assert np.array_equal(r1, r2)
+    codes = (r1[:, None] >> (4 * np.arange(8, dtype=np.uint32))) & 0xF
+    frac_n = (codes.ravel()[:1_000_000] == 4).mean()
+    assert 0.0 < frac_n < 0.01
+    s = mg.workload_spec(3, scale=0.0005, ref_size=100_000)
+    a = mg.make_workload(s, r1)
+    b = mg.make_workload(s, r1)
+    for k in ("peq", "qinfo", "cands"):
+        assert np.array_equal(a[k], b[k])
+    assert set(np.unique(a["lengths"])) <= {100, 200, 400, 600, 800, 1000}
+
+
+def test_synth_thread_independent(mg):
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, 'myers-gpu_b200'); import myersgpu as mg, numpy as np;"
+            "r = mg.make_reference(300_000, 9); w = mg.make_workload(mg.workload_spec(5, scale=0.002, ref_size=300_000), r);"
+            "print(int(r.sum() % 1000003), int(w['cands']['position'].sum() % 1000003), int(w['peq'].view(np.uint32).sum()))")
+    root = os.path.dirname(GOLDEN.rstrip("/")).rsplit("/", 1)[0]
+    outs = set()
+    for t in ("1", "3"):
+        env = dict(os.environ, OMP_NUM_THREADS=t)
+        outs.add(subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
+                                check=True).stdout)
+    assert len(outs) == 1
