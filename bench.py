@@ -166,10 +166,11 @@ def cpu_baseline(mg, k, args, full_cands):
         return sec
 
     # probe with a few reads, then size the sample to the time budget
+    total_reads = mg.workload_spec(k, scale=args.scale).num_reads
     s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0, num_reads=max(1, 2000 // (10 if k in (2, 4) else 1)))
     sec = max(run(w, ref_words, ref_size), 1e-4)
     per_read = sec / len(w["qinfo"])
-    n_reads = int(max(len(w["qinfo"]), min(s.num_reads, args.cpu_seconds / per_read)))
+    n_reads = int(max(len(w["qinfo"]), min(total_reads, args.cpu_seconds / per_read)))
     s.num_reads = n_reads
     w = mg.make_workload(s, ref_words)
     sec = run(w, ref_words, ref_size)
@@ -204,7 +205,8 @@ def run_reference(args):
         return time.perf_counter() - t
 
     sec = max(run(w), 1e-4)
-    s.num_reads = int(max(len(w["qinfo"]), min(s.num_reads, per_step / (sec / len(w["qinfo"])))))
+    total_reads = mg.workload_spec(k, scale=args.scale).num_reads
+    s.num_reads = int(max(len(w["qinfo"]), min(total_reads, per_step / (sec / len(w["qinfo"])))))
     w = mg.make_workload(s, ref_words)
     for _ in range(args.warmup):
         run(w)

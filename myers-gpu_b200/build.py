@@ -37,13 +37,19 @@ def build_cuda(verbose_ptxas=False):
     out = os.path.join(HERE, "libmyers_b200.so")
     srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
     deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [__file__]
+    extra =os.environ.get("MYERS_NVCC_FLAGS", "").split()  # e.g. -DMYERS_SHIFT_MODE=2
+    stamp = out + ".flags"
+    if os.path.exists(stamp) and open(stamp).read() != " ".join(extra):
+        os.remove(out)  # rebuild when the build options change
     if not _newer(out, deps) and not verbose_ptxas:
         return out
-    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared", *extra,
            "-I", os.path.join(ROOT, "include"), "-o", out, *srcs]
     if verbose_ptxas:
         cmd.insert(1, "-Xptxas=-v")
     _run(cmd)
+    with open(stamp, "w") as f:
+        f.write(" ".join(extra))
     return out
 
 

@@ -322,6 +322,8 @@ static int verify_enqueue(myersContext* ctx, const myersReference* ref, const De
   in.ref_size = ref->size;
   in.ref_words = ref->words + kRefPadWords;
   in.flags = ctx->d_flags;
+  in.one = 1u;
+  in.two = 2u;
   ctx->last_launches = 0;
   if (in.num_cands == 0) return MYERS_SUCCESS;
   if (in.num_cands > ctx->capacity) return MYERS_E_CAPACITY;
@@ -653,13 +655,10 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
   // O(queries) host pass: the word counts present pick the shapes
   std::vector<uint8_t>& present = b->present;
   std::fill(present.begin(), present.end(), 0);
-  bool too_long = false;
   for (uint32_t q = 0; q < numQueries; ++q) {
     const uint32_t m = b->h_qinfo[q].size;
-    if (m > kMaxWords * 32) too_long = true;
-    else if (m > 0) present[(m + 31) / 32] = 1;
+    if (m > 0 && m <= kMaxWords * 32) present[(m + 31) / 32] = 1;  // longer: flagged on the device
   }
-  (void)too_long;  // flagged on the device per candidate
   PlanTable& plan = b->plan;
   int st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
   if (st != MYERS_SUCCESS) return b->last_status = st;

@@ -88,6 +88,8 @@ struct DevInputs {
   uint32_t num_entries;
   float distance;
   int exact;
+  uint32_t one;                  // 1 and 2, set by the host: multipliers the
+  uint32_t two;                  // compiler cannot fold (see myers_kernels.cu)
 };
 
 inline int variant_W(int v) { return v < kNumSingle ? v + 1 : kMultiW[v - kNumSingle]; }

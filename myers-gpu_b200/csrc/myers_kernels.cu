@@ -70,8 +70,16 @@ __device__ __forceinline__ uint32_t qword(const uint32_t* __restrict__ peq, uint
                             : 0u;
 }
 
+// Shared-memory PEQ layout of one warp: [group g][base c][lane][4 words],
+// group g holding words 4g..4g+3 of a lane's W words. The eight lanes of one
+// LDS.128 phase always touch eight different 16-byte bank groups, whatever
+// bases they read, so the per-column loads are free of bank conflicts.
+constexpr int kLaneStride = 4;              // words between lanes
+constexpr int kBaseStride = 32 * 4;         // words between bases of a group
+constexpr int kGroupStride = 5 * 32 * 4;    // words between groups
+
 // Stage lane l's W words (of a 32*LW-row top-aligned query) for all five
-// bases: GW groups of [5 bases][4 words].
+// bases. `dst` = the warp's region + lane * kLaneStride.
 template <int W>
 __device__ __forceinline__ void stage_lane(uint32_t* __restrict__ dst, const uint32_t* __restrict__ peq,
                                            uint32_t pos_entry, uint32_t m, int LW, int l) {
@@ -91,17 +99,18 @@ __device__ __forceinline__ void stage_lane(uint32_t* __restrict__ dst, const uin
         uint32_t lo = qword(peq, pos_entry, nw, c, a - 1);
         v[j] = ps ? __funnelshift_r(lo, hi, 32 - ps) : hi;
       }
-      *reinterpret_cast<uint4*>(dst + (g * 5 + c) * 4) = make_uint4(v[0], v[1], v[2], v[3]);
+      *reinterpret_cast<uint4*>(dst + g * kGroupStride + c * kBaseStride) = make_uint4(v[0], v[1], v[2], v[3]);
     }
   }
 }
 
-// The W Eq words of one base; `p` points at the base's row of group 0.
+// The W Eq words of one base; `p` points at the lane's words of that base
+// in group 0.
 template <int W>
 __device__ __forceinline__ void load_eq(const uint32_t* __restrict__ p, uint32_t (&eq)[W]) {
 #pragma unroll
   for (int g = 0; g < (W + 3) / 4; ++g) {
-    const uint32_t* q = p + g * 20;
+    const uint32_t* q = p + g * kGroupStride;
     if (4 * g + 4 <= W) {
       uint4 v = *reinterpret_cast<const uint4*>(q);
       eq[4 * g] = v.x;
@@ -119,6 +128,16 @@ __device__ __forceinline__ void load_eq(const uint32_t* __restrict__ p, uint32_t
   }
 }
 
+#ifndef MYERS_SHIFT_MODE
+#define MYERS_SHIFT_MODE 0
+#endif
+
+// Multipliers 1 and 2 read from the kernel parameters: ptxas cannot fold them
+// into shifts or adds, so multiply-adds by them stay on the FMA pipe.
+struct Mul {
+  uint32_t one, two;
+};
+
 // s = a + b over W words with the carry rippling through the CC flag.
 template <int W>
 __device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t (&b)[W], uint32_t (&s)[W]) {
@@ -133,13 +152,27 @@ __device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t
   }
 }
 
+// (cur << 1) | (prev >> 31): the one-bit shift of a multi-word vector.
+// Mode 0 (default): one funnel shift on the ALU pipe. Mode 2: multiply-high
+// and multiply-add by an opaque two, on the FMA pipe -- fewer ALU
+// instructions but more instructions and latency in all; it loses at the
+// occupancy the single-lane shapes reach (measured).
+__device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k) {
+#if MYERS_SHIFT_MODE == 2
+  return cur * k.two + __umulhi(prev, k.two);
+#else
+  (void)k;
+  return __funnelshift_l(prev, cur, 1);
+#endif
+}
+
 // One text column over W words. With HIN, bit 31 of inP / inM is the
 // horizontal delta (+1 / -1) entering the bottom row (Myers' block rule);
 // without, it is 0 (semi-global: row 0 of the DP is all zeros).
 // topP / topM return the unshifted top words (bit 31 = delta out of the top row).
 template <int W, bool HIN>
 __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (&Pv)[W], uint32_t (&Mv)[W],
-                                             uint32_t inP, uint32_t inM, uint32_t& topP, uint32_t& topM) {
+                                             uint32_t inP, uint32_t inM, uint32_t& topP, uint32_t& topM, Mul k) {
   uint32_t e0 = eq[0];
   if (HIN) e0 |= inM >> 31;
   uint32_t t[W], s[W];
@@ -156,8 +189,8 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
     const uint32_t xh = (s[j] ^ pv) | e;
     const uint32_t ph = mv | ~(xh | pv);
     const uint32_t mh = pv & xh;
-    const uint32_t phs = __funnelshift_l(php, ph, 1);
-    const uint32_t mhs = __funnelshift_l(mhp, mh, 1);
+    const uint32_t phs = shl1(php, ph, k);
+    const uint32_t mhs = shl1(mhp, mh, k);
     Pv[j] = mhs | ~(xv | phs);
     Mv[j] = phs & xv;
     php = ph;
@@ -171,14 +204,14 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
 template <int W, bool TAIL>
 __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                               uint32_t (&Mv)[W], uint32_t& sc, uint32_t& kmin,
-                                              uint32_t colbase, uint32_t n) {
+                                              uint32_t colbase, uint32_t n, Mul k) {
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const uint32_t off = ((t >> (4 * u)) & 7u) << 4;
+    const uint32_t off = ((t >> (4 * u)) & 7u) << 9;  // base * kBaseStride * 4 bytes
     uint32_t eq[W];
     load_eq<W>(reinterpret_cast<const uint32_t*>(slot + off), eq);
     uint32_t tp, tm;
-    myers_column<W, false>(eq, Pv, Mv, 0u, 0u, tp, tm);
+    myers_column<W, false>(eq, Pv, Mv, 0u, 0u, tp, tm, k);
     sc += (tp >> 31) << 16;
     sc -= (tm >> 31) << 16;
     const uint32_t key = sc + colbase + (uint32_t)u;
@@ -245,16 +278,13 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
 template <int W, bool MULTI>
 __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
                                              uint32_t cnt, int L, uint32_t* __restrict__ wsmem, int lane) {
-  constexpr int GW = (W + 3) / 4;
   const int Lr = MULTI ? L : 1;
   const int nseg = MULTI ? 32 / L : 32;
   const int seg = MULTI ? lane / L : lane;
   const int l = MULTI ? lane - seg * L : 0;
   const int LW = Lr * W;
   const int rows = 32 * LW;
-  // lanes past the last segment (L not dividing 32) read segment 0's slot
-  const int sseg = seg < nseg ? seg : 0;
-  uint32_t* lane_part = wsmem + (sseg * Lr + l) * GW * 20;
+  uint32_t* lane_part = wsmem + lane * kLaneStride;
 
   const CandSetup c = setup_candidate(in, ids, first, cnt, seg, nseg, l, rows);
   if (c.work) stage_lane<W>(lane_part, in.peq, c.pos_entry, c.m, LW, l);
@@ -273,6 +303,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
   const long long b0 = q0 >> 3;
   const uint32_t sh = 4u * (uint32_t)(q0 & 7);
   const char* slot = reinterpret_cast<const char*>(lane_part);
+  const Mul k{in.one, in.two};
 
   if constexpr (!MULTI) {
     if (c.work) {
@@ -284,11 +315,11 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
         const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
         lo = hi;
         hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
-        block8_single<W, false>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n);
+        block8_single<W, false>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n, k);
       }
       if (c.n & 7u) {
         const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
-        block8_single<W, true>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n);
+        block8_single<W, true>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n, k);
       }
       in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
     }
@@ -306,7 +337,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
       hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        const uint32_t off = ((t >> (4 * u)) & 7u) << 4;
+        const uint32_t off = ((t >> (4 * u)) & 7u) << 9;
         uint32_t eq[W];
         load_eq<W>(reinterpret_cast<const uint32_t*>(slot + off), eq);
         uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1);
@@ -317,7 +348,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
         }
         const uint32_t j = 8u * i + (uint32_t)u - (uint32_t)l;  // wraps when negative
         if (c.work && j < c.n) {
-          myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM);
+          myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM, k);
           sc += (outP >> 31) << 16;
           sc -= (outM >> 31) << 16;
           kmin = min(kmin, sc + j);
@@ -329,9 +360,9 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
   __syncwarp();
 }
 
-template <int W, bool MULTI>
-__host__ __device__ constexpr uint32_t warp_words(int L) {
-  return (uint32_t)((MULTI ? (32 / L) * L : 32) * ((W + 3) / 4) * 20);
+template <int W>
+__host__ __device__ constexpr uint32_t warp_words() {
+  return (uint32_t)(((W + 3) / 4) * kGroupStride);
 }
 
 // Plain launch: one shape over a contiguous range of (sorted) candidates,
@@ -347,7 +378,7 @@ __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __r
     count = st->count[cfg];
   }
   const int nseg = MULTI ? 32 / L : 32;
-  uint32_t* wsmem = smem + wib * warp_words<W, MULTI>(L);
+  uint32_t* wsmem = smem + wib * warp_words<W>();
   const uint32_t tiles = (count + nseg - 1) / nseg;
   const uint32_t wpb = blockDim.x >> 5;
   for (uint32_t t = blockIdx.x * wpb + wib; t < tiles; t += gridDim.x * wpb) {
@@ -436,7 +467,7 @@ __global__ void k_scatter(uint32_t n, const uint8_t* __restrict__ cfg_of_cand, B
 
 // ---- the persistent batched kernel ----
 
-constexpr uint32_t kBatchedWarpWords = 32 * ((kBatchedMaxW + 3) / 4) * 20;  // the largest batched shape
+constexpr uint32_t kBatchedWarpWords = warp_words<kBatchedMaxW>();  // the largest batched shape
 
 template <int V>
 __device__ __forceinline__ void dispatch_one(const DevInputs& in, const uint32_t* ids, uint32_t f, uint32_t cnt,
@@ -538,11 +569,9 @@ constexpr auto make_plain_table(std::integer_sequence<int, Vs...>) {
 
 static const auto kPlainTable = make_plain_table(std::make_integer_sequence<int, kNumVariants>{});
 
-uint32_t warp_smem_bytes(int v, int L) {
+uint32_t warp_smem_bytes(int v, int) {
   const int W = variant_W(v);
-  const int gw = (W + 3) / 4;
-  const int lanes = variant_multi(v) ? (32 / L) * L : 32;
-  return (uint32_t)(lanes * gw * 20 * 4);
+  return (uint32_t)(((W + 3) / 4) * kGroupStride * 4);
 }
 
 static int blocks_per_sm(const void* fn, int threads, size_t smem) {
