@@ -211,46 +211,53 @@ static Shape pick_shape(uint32_t w, bool batched) {
 }
 
 // Build the plan for the word counts flagged in `present` (size kMaxWords+1).
+// Uses fixed-size stack arrays only: no allocation on the send path.
 static int build_plan(PlanTable& t, const uint8_t* present, bool batched) {
   memset(&t, 0, sizeof(t));
   memset(t.cfg_of_words, kNoCfg, sizeof(t.cfg_of_words));
-  struct Entry {
-    Shape s;
-    uint32_t max_words;
-  };
-  std::vector<Entry> shapes;
-  std::vector<int> cfg_of(kMaxWords + 1, -1);
+  Shape shapes[kMaxCfg];
+  uint32_t max_words[kMaxCfg];
+  int16_t cfg_of[kMaxWords + 1];
+  int nshapes = 0;
+  for (uint32_t w = 0; w <= kMaxWords; ++w) cfg_of[w] = -1;
   for (uint32_t w = 1; w <= kMaxWords; ++w) {
     if (!present[w]) continue;
     const Shape s = pick_shape(w, batched);
     if (s.L == 0) return MYERS_E_QUERY_TOO_LONG;
     int found = -1;
-    for (size_t i = 0; i < shapes.size(); ++i)
-      if (shapes[i].s.variant == s.variant && shapes[i].s.L == s.L) found = (int)i;
+    for (int i = 0; i < nshapes; ++i)
+      if (shapes[i].variant == s.variant && shapes[i].L == s.L) found = i;
     if (found < 0) {
-      shapes.push_back(Entry{s, w});
-      found = (int)shapes.size() - 1;
+      if (nshapes == kMaxCfg) return MYERS_E_QUERY_TOO_LONG;
+      shapes[nshapes] = s;
+      max_words[nshapes] = w;
+      found = nshapes++;
     }
-    if (w > shapes[found].max_words) shapes[found].max_words = w;
-    cfg_of[w] = found;
+    if (w > max_words[found]) max_words[found] = w;
+    cfg_of[w] = (int16_t)found;
   }
-  if (shapes.size() > (size_t)kMaxCfg) return MYERS_E_QUERY_TOO_LONG;
   // order: persistent-kernel shapes first, each group by decreasing cost
-  std::vector<int> order(shapes.size());
-  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-  auto key = [&](int i) {
-    const bool b = batched_supports(shapes[i].s.variant);
-    const double cost = shape_cost(shapes[i].s.variant, shapes[i].s.L) * shapes[i].max_words;
-    return std::make_pair(b ? 0 : 1, -cost);
-  };
-  for (size_t i = 1; i < order.size(); ++i)
-    for (size_t j = i; j > 0 && key(order[j]) < key(order[j - 1]); --j) std::swap(order[j], order[j - 1]);
-  std::vector<int> rank(shapes.size());
-  t.num_cfg = (uint32_t)shapes.size();
+  int order[kMaxCfg];
+  double cost[kMaxCfg];
+  bool group[kMaxCfg];
+  for (int i = 0; i < nshapes; ++i) {
+    order[i] = i;
+    group[i] = !batched_supports(shapes[i].variant);
+    cost[i] = shape_cost(shapes[i].variant, shapes[i].L) * max_words[i];
+  }
+  auto before = [&](int a, int b) { return group[a] != group[b] ? group[a] < group[b] : cost[a] > cost[b]; };
+  for (int i = 1; i < nshapes; ++i)
+    for (int j = i; j > 0 && before(order[j], order[j - 1]); --j) {
+      const int x = order[j];
+      order[j] = order[j - 1];
+      order[j - 1] = x;
+    }
+  int rank[kMaxCfg];
+  t.num_cfg = (uint32_t)nshapes;
   t.num_batched = 0;
-  for (size_t r = 0; r < order.size(); ++r) {
-    rank[order[r]] = (int)r;
-    t.shape[r] = shapes[order[r]].s;
+  for (int r = 0; r < nshapes; ++r) {
+    rank[order[r]] = r;
+    t.shape[r] = shapes[order[r]];
     if (batched_supports(t.shape[r].variant)) t.num_batched = (uint32_t)r + 1;
   }
   for (uint32_t w = 1; w <= kMaxWords; ++w)
@@ -357,12 +364,13 @@ static int verify_enqueue(myersContext* ctx, const myersReference* ref, const De
 }
 
 static int plan_for_range(PlanTable& plan, uint32_t minSize, uint32_t maxSize, int path) {
-  std::vector<uint8_t> present(kMaxWords + 1, 0);
+  uint8_t present[kMaxWords + 1];
+  memset(present, 0, sizeof(present));
   if (maxSize == 0) maxSize = kMaxWords * 32;
   if (maxSize > kMaxWords * 32) maxSize = kMaxWords * 32;
   const uint32_t wlo = minSize ? (minSize + 31) / 32 : 1, whi = (maxSize + 31) / 32;
   for (uint32_t w = wlo; w <= whi; ++w) present[w] = 1;
-  return build_plan(plan, present.data(), path == MYERS_PATH_BATCHED);
+  return build_plan(plan, present, path == MYERS_PATH_BATCHED);
 }
 
 extern "C" int myersVerifyAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
