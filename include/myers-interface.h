@@ -219,6 +219,39 @@ int myersVerifyRangeAsync(myersContext_t *ctx, const myersReference_t *ref,
                           uint32_t minQuerySize, uint32_t maxQuerySize,
                           resEntry_t *d_results, void *stream);
 
+/* Largest batch myersVerifyNoAllocAsync accepts (candidates). */
+#define MYERS_NOALLOC_MAX_CANDIDATES 262144u
+
+/* Verification that allocates nothing. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code that runs while a stream is
+ * being captured into a CUDA graph, programs whose allocator owns all of
+ * device memory (a caching allocator or an arena carved out at start-up), and
+ * services whose memory budget is frozen once they are up. Inputs and outputs
+ * are the caller's device memory, as for myersVerifyRangeAsync, and the
+ * reference is passed as raw device words (refWords readable words holding
+ * refSizeBases bases; reads past them act as N). It runs the batched path;
+ * its scratch lives in a device array inside this library, about 1.3 MB,
+ * that every GPU which loads the library holds until the process exits.
+ *
+ *  - at most MYERS_NOALLOC_MAX_CANDIDATES candidates per call; larger batches
+ *    return MYERS_E_CAPACITY and enqueue nothing;
+ *  - the first call on a device resolves the array's device address (with
+ *    that device current); make that first call before any stream capture;
+ *  - every call on a device shares the one array and leaves its contents
+ *    behind (each call clears what must start at zero): calls that overlap on
+ *    the GPU (other streams, or other threads) race and give wrong results;
+ *    serialise them, e.g. on one stream;
+ *  - error flags are not reported: flagged candidates get {0, 0xFFFFFFFF}.
+ * Asynchronous on `stream` (a cudaStream_t). */
+int myersVerifyNoAllocAsync(const uint32_t *d_refWords, uint64_t refWords, uint64_t refSizeBases,
+                            const qryEntry_t *d_peq, uint32_t numPEQEntries,
+                            const qryInfo_t *d_qinfo, uint32_t numQueries,
+                            const candInfo_t *d_cands, uint32_t numCandidates,
+                            float distance, int windowMode,
+                            uint32_t minQuerySize, uint32_t maxQuerySize,
+                            resEntry_t *d_results, void *stream);
+
 /* Kernel launches the last myersVerify*Async on this context enqueued. */
 uint32_t myersContextLastLaunches(const myersContext_t *ctx);
 

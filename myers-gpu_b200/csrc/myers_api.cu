@@ -744,3 +744,114 @@ extern "C" int myersGetLastStatus(void* mb) { return mb ? static_cast<Buffer*>(m
 extern "C" uint32_t myersBufferLastLaunches(void* mb) {
   return mb ? static_cast<Buffer*>(mb)->ctx->last_launches : 0;
 }
+
+// ---------------------------------------------------------------------------
+// Verification that allocates nothing (no counterpart in the reference).
+//
+// Some callers cannot call cudaMalloc: code running while a stream is being
+// captured into a CUDA graph, allocators that own all of device memory
+// (a caching allocator or a fixed arena handed out once), and services whose
+// memory budget is frozen after start-up. For them this entry point runs the
+// batched path with its bucketing scratch (candidate ids sorted by shape, a
+// shape byte per candidate, the bucket table and the error flags) in the
+// file-scope device array below instead of a context's allocations. The
+// array is sized for MYERS_NOALLOC_MAX_CANDIDATES candidates (about 1.3 MB)
+// and every GPU that loads this library holds it until the process exits.
+
+constexpr uint32_t kNoAllocMax = MYERS_NOALLOC_MAX_CANDIDATES;
+constexpr size_t kNoAllocStateBytes = (sizeof(BucketState) + 255) & ~(size_t)255;
+constexpr size_t kNoAllocIdsOffset = kNoAllocStateBytes;
+constexpr size_t kNoAllocCfgOffset = kNoAllocIdsOffset + (size_t)kNoAllocMax * 4;
+constexpr size_t kNoAllocFlagsOffset = kNoAllocCfgOffset + (((size_t)kNoAllocMax + 255) & ~(size_t)255);
+constexpr size_t kNoAllocBytes = kNoAllocFlagsOffset + 256;
+
+// Host code must not use this name as a device address: on the host it is a
+// stand-in symbol. Its device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+  bool ready;
+  unsigned char* scratch;  // device address of g_noalloc_scratch on this device
+  int num_sms;
+};
+static std::mutex g_noalloc_mu;
+static NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+// Once per device, with that device current: resolve the array's device
+// address (this may load the module, so it should not happen inside a
+// stream capture; the first call on each device does it).
+static int noalloc_setup(NoAllocDevice* out) {
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return MYERS_E_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    d.scratch = static_cast<unsigned char*>(p);
+    d.num_sms = sms;
+    d.ready = true;
+  }
+  *out = d;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refWords, uint64_t refSizeBases,
+                                       const qryEntry_t* d_peq, uint32_t numPEQEntries,
+                                       const qryInfo_t* d_qinfo, uint32_t numQueries,
+                                       const candInfo_t* d_cands, uint32_t numCandidates, float distance,
+                                       int windowMode, uint32_t minQuerySize, uint32_t maxQuerySize,
+                                       resEntry_t* d_results, void* stream) {
+  if (!(distance >= 0.0f) || !std::isfinite(distance)) return MYERS_E_INVALID_ARGUMENT;
+  if (windowMode != MYERS_WINDOW_ALIGNED && windowMode != MYERS_WINDOW_EXACT) return MYERS_E_INVALID_ARGUMENT;
+  if (refSizeBases > refWords * 8) return MYERS_E_INVALID_ARGUMENT;
+  if (numCandidates > kNoAllocMax) return MYERS_E_CAPACITY;  // beyond the static scratch
+  if (numCandidates == 0) return MYERS_SUCCESS;
+  if (d_refWords == nullptr || d_peq == nullptr || d_qinfo == nullptr || d_cands == nullptr || d_results == nullptr)
+    return MYERS_E_INVALID_ARGUMENT;
+  NoAllocDevice dev;
+  int st = noalloc_setup(&dev);
+  if (st != MYERS_SUCCESS) return st;
+  PlanTable plan;
+  st = plan_for_range(plan, minQuerySize, maxQuerySize, MYERS_PATH_BATCHED);
+  if (st != MYERS_SUCCESS) return st;
+  BucketState* d_state = reinterpret_cast<BucketState*>(dev.scratch);
+  uint32_t* d_ids = reinterpret_cast<uint32_t*>(dev.scratch + kNoAllocIdsOffset);
+  uint8_t* d_cfg = dev.scratch + kNoAllocCfgOffset;
+  uint32_t* d_flags = reinterpret_cast<uint32_t*>(dev.scratch + kNoAllocFlagsOffset);
+  DevInputs in;
+  memset(&in, 0, sizeof(in));
+  in.peq = reinterpret_cast<const uint32_t*>(d_peq);
+  in.qinfo = reinterpret_cast<const uint2*>(d_qinfo);
+  in.cands = reinterpret_cast<const Cand*>(d_cands);
+  in.ref = d_refWords;
+  in.ref_size = refSizeBases;
+  in.ref_words = refWords;
+  in.results = reinterpret_cast<uint2*>(d_results);
+  in.flags = d_flags;
+  in.num_cands = numCandidates;
+  in.num_queries = numQueries;
+  in.num_entries = numPEQEntries;
+  in.distance = distance;
+  in.exact = windowMode == MYERS_WINDOW_EXACT;
+  in.one = 1u;
+  in.two = 2u;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the array keeps the previous call's contents: the bucket table (counts,
+  // cursors, work queue) and the flags must start at zero
+  CU(cudaMemsetAsync(d_state, 0, sizeof(BucketState), s));
+  CU(cudaMemsetAsync(d_flags, 0, sizeof(uint32_t), s));
+  cudaError_t e = cudaSuccess;
+  launch_bucketing(in, plan, d_state, d_cfg, d_ids, s, dev.num_sms, &e);
+  if (e != cudaSuccess) return cuda_fail(e, "bucketing");
+  if (plan.num_batched > 0) CU(launch_batched(in, d_ids, plan, d_state, s, dev.num_sms));
+  for (uint32_t c = plan.num_batched; c < plan.num_cfg; ++c)
+    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, d_ids, d_state, (int)c, 0, 0, s, dev.num_sms));
+  return MYERS_SUCCESS;
+}

@@ -34,6 +34,7 @@ WINDOW_ALIGNED, WINDOW_EXACT = 0, 1
 PATH_PLAIN, PATH_BATCHED = 0, 1
 NO_RESULT = 0xFFFFFFFF
 MAX_QUERY_BASES = 32768
+NOALLOC_MAX_CANDIDATES = 262144
 
 
 class MyersError(RuntimeError):
@@ -85,6 +86,7 @@ _sig("myersContextCreate", _I32, _PP, _U64)
 _sig("myersContextDestroy", _I32, _P)
 _sig("myersVerifyAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _P, _P)
 _sig("myersVerifyRangeAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _U32, _U32, _P, _P)
+_sig("myersVerifyNoAllocAsync", _I32, _P, _U64, _U64, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _U32, _U32, _P, _P)
 _sig("myersContextLastLaunches", _U32, _P)
 _sig("myersContextFlags", _I32, _P, C.POINTER(_U32), _I32)
 _sig("myersNumVariants", _I32)
@@ -101,7 +103,7 @@ EXPORTED = (
     "myersGetErrorString myersInit myersSend myersReceive myersEnd myersSetWindowMode "
     "myersSetKernelPath myersSetMemoryBudget myersGetDevice myersGetLastStatus myersReferenceCreate "
     "myersReferenceLoad myersReferenceDestroy myersReferenceSize myersContextCreate myersContextDestroy "
-    "myersVerifyAsync myersVerifyRangeAsync myersContextLastLaunches myersContextFlags "
+    "myersVerifyAsync myersVerifyRangeAsync myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
     "myersBufferLastLaunches myersNumVariants myersVariantWords myersVariantIsMulti myersShapeOf "
     "myersSetShapeOverride myersProbeIntPeak"
 ).split()
