@@ -264,6 +264,73 @@ int myersContextFlags(myersContext_t *ctx, uint32_t *flags, int clear);
 uint32_t myersBufferLastLaunches(void *myersBuffer);
 
 /* ---------------------------------------------------------------------------
+ * Serving loop (no counterpart in the reference): requests -- one read and
+ * its candidate positions -- are admitted under a device-memory budget and
+ * verified in batches that form continuously: while some batches are on the
+ * GPU, requests that arrive are gathered into the next batch, which starts as
+ * soon as a batch slot frees up. Each slot has its own stream, so copies and
+ * kernels of consecutive batches overlap on the device. The reference stays
+ * resident.
+ * ------------------------------------------------------------------------- */
+
+typedef struct myersServer myersServer_t;
+
+typedef struct {
+    uint64_t budgetBytes;        /* device memory of all batch slots (0: 16 GiB, capped at 80% of free) */
+    uint32_t slots;              /* batches in flight (0: 4) */
+    uint32_t maxBatchCandidates; /* per batch slot (0: 1<<20, lowered to fit the budget) */
+    uint32_t maxQueued;          /* requests waiting for a slot before submit refuses (0: 1<<20) */
+    float distance;              /* error fraction, as sendMyersBuffer */
+    int windowMode;              /* MYERS_WINDOW_* */
+    int path;                    /* MYERS_PATH_* (default batched) */
+    uint32_t maxQuerySize;       /* longest read accepted (0: 1024 bases) */
+    uint32_t laneWords;          /* 0: throughput shapes; k > 0: spread a read of more than k
+                                    32-bit words over several lanes of >= k words each, which
+                                    cuts its time on the GPU (latency) for a few percent more work */
+    int useGraphs;               /* non-zero: capture each batch's copies and kernels and replay them
+                                    as a CUDA graph (updated in place batch to batch) */
+} myersServerConfig_t;
+
+typedef struct {
+    uint64_t submitted, refused, completed, batches;
+    uint64_t batchCandidatesMax;  /* largest batch dispatched */
+    uint64_t candidatesCompleted;
+    uint32_t slots, maxBatchCandidates, maxBatchQueries, maxBatchEntries;
+} myersServerStats_t;
+
+int myersServerCreate(myersServer_t **srv, const myersReference_t *ref, const myersServerConfig_t *cfg);
+
+/* Queue one request: `peq` holds the read's ceil(querySize/128) PEQ entries,
+ * `positions` its numCandidates reference positions. Copies both. Returns
+ * MYERS_E_BUSY when maxQueued requests already wait, MYERS_E_CAPACITY when
+ * the request alone exceeds a batch slot. */
+int myersServerSubmit(myersServer_t *srv, const qryEntry_t *peq, uint32_t querySize,
+                      const uint64_t *positions, uint32_t numCandidates, uint64_t *ticket);
+
+/* MYERS_E_NOT_READY until the request is done; then copies its numCandidates
+ * results (candidate order) into `results` and forgets the ticket. */
+int myersServerPoll(myersServer_t *srv, uint64_t ticket, resEntry_t *results);
+
+/* Block until the request is done (or timeoutMs passes: MYERS_E_TIMEOUT). */
+int myersServerWait(myersServer_t *srv, uint64_t ticket, resEntry_t *results, uint32_t timeoutMs);
+
+int myersServerStats(myersServer_t *srv, myersServerStats_t *stats);
+
+/* Stop accepting, finish what is in flight, free everything. */
+int myersServerDestroy(myersServer_t *srv);
+
+/* Open-loop load for measurement: request i (read qinfo[i], PEQ entries from
+ * qinfo[i].posEntry, candidates positions[candOffset[i] .. candOffset[i+1]))
+ * is submitted at arrivalNs[i] after the start by a driver thread, whatever
+ * the server's state. latencyNs[i] = completion - scheduled arrival
+ * (UINT64_MAX if refused); results receive every candidate's result in
+ * request order. *wallNs = first arrival to last completion. */
+int myersServerReplay(myersServer_t *srv, const qryEntry_t *peq, const qryInfo_t *qinfo,
+                      const uint32_t *candOffset, const uint64_t *positions, uint32_t numRequests,
+                      const uint64_t *arrivalNs, uint64_t *latencyNs, resEntry_t *results,
+                      uint64_t *wallNs);
+
+/* ---------------------------------------------------------------------------
  * Kernel shapes (autotuning)
  * ------------------------------------------------------------------------- */
 

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["myers_kernels.cu", "myers_api.cu"]
+CUDA_SOURCES = ["myers_kernels.cu", "myers_api.cu", "myers_serve.cu"]
 CUDA_HEADERS = ["myers_internal.h", os.path.join("..", "..", "include", "myers-interface.h")]
 
 

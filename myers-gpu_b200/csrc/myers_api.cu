@@ -40,7 +40,7 @@ static_assert(sizeof(Cand) == 16, "Cand layout");
 
 static thread_local char g_cuda_msg[256];
 
-static int cuda_fail(cudaError_t e, const char* what) {
+int myers::cuda_fail(cudaError_t e, const char* what) {
   snprintf(g_cuda_msg, sizeof(g_cuda_msg), "%s: %s", what, cudaGetErrorString(e));
   return MYERS_E_CUDA;
 }
@@ -81,12 +81,6 @@ static void fatal(int status, const char* where) {
 // ---------------------------------------------------------------------------
 // reference
 
-struct myersReference {
-  int device;
-  uint32_t* d_words;
-  uint64_t words;  // packed words (without padding)
-  uint64_t size;   // bases
-};
 
 static int reference_upload(myersReference** out, const uint32_t* host, uint64_t words, uint64_t size) {
   if (out == nullptr || (words > 0 && host == nullptr)) return MYERS_E_INVALID_ARGUMENT;
@@ -185,11 +179,23 @@ struct Override {
 static std::mutex g_override_mu;
 static Override g_override[2][kMaxWords + 1];
 
-static Shape pick_shape(uint32_t w, bool batched) {
+// lane_words > 0 asks for latency-oriented shapes: a query of more than
+// lane_words words is spread over ceil(words / W) lanes, W the smallest
+// multi-lane width >= lane_words (shorter per-candidate time, a few percent
+// more instructions).
+static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
   {
     std::lock_guard<std::mutex> lk(g_override_mu);
     const Override& o = g_override[batched ? 1 : 0][w];
     if (o.set) return Shape{o.variant, o.L, (uint8_t)variant_W(o.variant), 0};
+  }
+  if (lane_words > 0 && w > lane_words) {
+    for (int mi = 0; mi < kNumMulti; ++mi) {
+      const uint32_t W = (uint32_t)kMultiW[mi];
+      if (W < lane_words || (batched && W > (uint32_t)kBatchedMaxW)) continue;
+      const uint32_t L = (w + W - 1) / W;
+      if (L >= 2 && L <= 32) return Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};
+    }
   }
   const uint32_t single_max = batched ? (uint32_t)kBatchedMaxW : 32u;
   if (w <= single_max) return Shape{(uint8_t)(w - 1), 1, (uint8_t)w, 0};
@@ -212,7 +218,7 @@ static Shape pick_shape(uint32_t w, bool batched) {
 
 // Build the plan for the word counts flagged in `present` (size kMaxWords+1).
 // Uses fixed-size stack arrays only: no allocation on the send path.
-static int build_plan(PlanTable& t, const uint8_t* present, bool batched) {
+int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words) {
   memset(&t, 0, sizeof(t));
   memset(t.cfg_of_words, kNoCfg, sizeof(t.cfg_of_words));
   Shape shapes[kMaxCfg];
@@ -222,7 +228,7 @@ static int build_plan(PlanTable& t, const uint8_t* present, bool batched) {
   for (uint32_t w = 0; w <= kMaxWords; ++w) cfg_of[w] = -1;
   for (uint32_t w = 1; w <= kMaxWords; ++w) {
     if (!present[w]) continue;
-    const Shape s = pick_shape(w, batched);
+    const Shape s = pick_shape(w, batched, lane_words);
     if (s.L == 0) return MYERS_E_QUERY_TOO_LONG;
     int found = -1;
     for (int i = 0; i < nshapes; ++i)
@@ -268,16 +274,6 @@ static int build_plan(PlanTable& t, const uint8_t* present, bool batched) {
 // ---------------------------------------------------------------------------
 // context: device scratch for bucketing
 
-struct myersContext {
-  int device;
-  int num_sms;
-  uint64_t capacity;
-  uint32_t* d_ids;
-  uint8_t* d_cfg;
-  BucketState* d_state;
-  uint32_t* d_flags;
-  uint32_t last_launches;
-};
 
 extern "C" int myersContextCreate(myersContext_t** out, uint64_t maxCandidates) {
   if (out == nullptr || maxCandidates > 0xFFFFFFFFull) return MYERS_E_INVALID_ARGUMENT;
@@ -322,7 +318,20 @@ extern "C" uint32_t myersContextLastLaunches(const myersContext_t* c) { return c
 
 // Enqueue the kernels for one batch. `uniform`: every query maps to the same
 // (single) shape of `plan`, so no bucketing is needed on the plain path.
-static int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in0, const PlanTable& plan,
+// Most work tiles the persistent kernel can see for n candidates: every
+// candidate in the shape with the fewest candidates per tile, plus one
+// partial tile per shape.
+uint32_t myers::batched_tile_bound(const PlanTable& plan, uint32_t n) {
+  uint32_t nseg_min = 32;
+  for (uint32_t c = 0; c < plan.num_batched; ++c) {
+    const Shape sh = plan.shape[c];
+    const uint32_t nseg = variant_multi(sh.variant) ? 32u / sh.L : 32u;
+    if (nseg < nseg_min) nseg_min = nseg;
+  }
+  return (uint32_t)(((uint64_t)n + nseg_min - 1) / nseg_min + plan.num_batched);
+}
+
+int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in0, const PlanTable& plan,
                           int path, cudaStream_t s) {
   DevInputs in = in0;
   in.ref = ref->d_words;
@@ -350,7 +359,7 @@ static int verify_enqueue(myersContext* ctx, const myersReference* ref, const De
   if (e != cudaSuccess) return cuda_fail(e, "bucketing");
   uint32_t first_plain = 0;
   if (path == MYERS_PATH_BATCHED && plan.num_batched > 0) {
-    CU(launch_batched(in, ctx->d_ids, plan, ctx->d_state, s, ctx->num_sms));
+    CU(launch_batched(in, ctx->d_ids, plan, ctx->d_state, s, ctx->num_sms, batched_tile_bound(plan, in.num_cands)));
     ++launches;
     first_plain = plan.num_batched;
   }
@@ -850,7 +859,8 @@ extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refW
   cudaError_t e = cudaSuccess;
   launch_bucketing(in, plan, d_state, d_cfg, d_ids, s, dev.num_sms, &e);
   if (e != cudaSuccess) return cuda_fail(e, "bucketing");
-  if (plan.num_batched > 0) CU(launch_batched(in, d_ids, plan, d_state, s, dev.num_sms));
+  if (plan.num_batched > 0)
+    CU(launch_batched(in, d_ids, plan, d_state, s, dev.num_sms, batched_tile_bound(plan, numCandidates)));
   for (uint32_t c = plan.num_batched; c < plan.num_cfg; ++c)
     CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, d_ids, d_state, (int)c, 0, 0, s, dev.num_sms));
   return MYERS_SUCCESS;

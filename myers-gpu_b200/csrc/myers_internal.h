@@ -108,9 +108,12 @@ int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_
 cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
                          int cfg, uint32_t first, uint32_t count, cudaStream_t s, int num_sms);
 
-// The persistent batched launch over the plan's first num_batched shapes.
+// The persistent batched launch over the plan's first num_batched shapes;
+// the grid is the device's resident capacity or, for small batches, one
+// warp per tile of `max_tiles` (an upper bound of the tiles), whichever is
+// smaller, so concurrent small batches share the device.
 cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,
-                           BucketState* d_state, cudaStream_t s, int num_sms);
+                           BucketState* d_state, cudaStream_t s, int num_sms, uint32_t max_tiles);
 
 // Bytes of shared memory one warp needs for a shape.
 uint32_t warp_smem_bytes(int v, int L);
@@ -118,4 +121,38 @@ uint32_t warp_smem_bytes(int v, int L);
 // Integer-ALU peak probe: `iters` rounds of independent 3-input logic ops.
 cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iters, cudaStream_t s);
 
+// ---- host runtime internals (myers_api.cu) ----
+
+// Shape plan for the word counts flagged in present[0..kMaxWords].
+int build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words = 0);
+// Upper bound of the persistent kernel's tiles for n candidates under `plan`.
+uint32_t batched_tile_bound(const PlanTable& plan, uint32_t n);
+// Record a CUDA failure (message for myersGetErrorString) and return MYERS_E_CUDA.
+int cuda_fail(cudaError_t e, const char* what);
+
+}  // namespace myers
+
+// Opaque handles of the C ABI (include/myers-interface.h).
+struct myersReference {
+  int device;
+  uint32_t* d_words;
+  uint64_t words;  // packed words (without padding)
+  uint64_t size;   // bases
+};
+
+struct myersContext {
+  int device;
+  int num_sms;
+  uint64_t capacity;
+  uint32_t* d_ids;
+  uint8_t* d_cfg;
+  myers::BucketState* d_state;
+  uint32_t* d_flags;
+  uint32_t last_launches;
+};
+
+namespace myers {
+// Enqueue the kernels of one batch on stream s (inputs already on the device).
+int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in, const PlanTable& plan, int path,
+                   cudaStream_t s);
 }  // namespace myers

@@ -615,14 +615,17 @@ int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_
 }
 
 cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,
-                           BucketState* d_state, cudaStream_t s, int num_sms) {
+                           BucketState* d_state, cudaStream_t s, int num_sms, uint32_t max_tiles) {
   const int threads = 128;
   const size_t smem = (size_t)kBatchedWarpWords * 4 * (threads / 32);
   cudaError_t e = cudaFuncSetAttribute((const void*)k_batched, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   const int nb = blocks_per_sm((const void*)k_batched, threads, smem);
-  k_batched<<<num_sms * nb, threads, smem, s>>>(in, d_ids, plan, d_state);
+  uint32_t grid = (uint32_t)(num_sms * nb);
+  const uint32_t need = (max_tiles + threads / 32 - 1) / (threads / 32);
+  if (need < grid) grid = need > 0 ? need : 1;
+  k_batched<<<grid, threads, smem, s>>>(in, d_ids, plan, d_state);
   return cudaGetLastError();
 }
 

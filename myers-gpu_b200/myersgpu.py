@@ -88,6 +88,13 @@ _sig("myersVerifyAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _
 _sig("myersVerifyRangeAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _U32, _U32, _P, _P)
 _sig("myersVerifyNoAllocAsync", _I32, _P, _U64, _U64, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _U32, _U32, _P, _P)
 _sig("myersContextLastLaunches", _U32, _P)
+_sig("myersServerCreate", _I32, _PP, _P, _P)
+_sig("myersServerSubmit", _I32, _P, _P, _U32, _P, _U32, C.POINTER(_U64))
+_sig("myersServerPoll", _I32, _P, _U64, _P)
+_sig("myersServerWait", _I32, _P, _U64, _P, _U32)
+_sig("myersServerStats", _I32, _P, _P)
+_sig("myersServerDestroy", _I32, _P)
+_sig("myersServerReplay", _I32, _P, _P, _P, _P, _P, _U32, _P, _P, _P, C.POINTER(_U64))
 _sig("myersContextFlags", _I32, _P, C.POINTER(_U32), _I32)
 _sig("myersNumVariants", _I32)
 _sig("myersVariantWords", _I32, _I32)
@@ -105,7 +112,8 @@ EXPORTED = (
     "myersReferenceLoad myersReferenceDestroy myersReferenceSize myersContextCreate myersContextDestroy "
     "myersVerifyAsync myersVerifyRangeAsync myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
     "myersBufferLastLaunches myersNumVariants myersVariantWords myersVariantIsMulti myersShapeOf "
-    "myersSetShapeOverride myersProbeIntPeak"
+    "myersSetShapeOverride myersProbeIntPeak myersServerCreate myersServerSubmit myersServerPoll myersServerWait "
+    "myersServerStats myersServerDestroy myersServerReplay"
 ).split()
 
 
@@ -282,6 +290,82 @@ def verify_torch(ctx, ref, peq, qinfo, cands, distance, window=WINDOW_ALIGNED, p
                d_res.data_ptr(), window=window, path=path, stream=stream, min_size=min_size, max_size=max_size)
     torch.cuda.synchronize()
     return d_res.cpu().numpy().view(RES)
+
+
+# ---------------------------------------------------------------------------
+# serving loop
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("budgetBytes", C.c_uint64), ("slots", C.c_uint32), ("maxBatchCandidates", C.c_uint32),
+                ("maxQueued", C.c_uint32), ("distance", C.c_float), ("windowMode", C.c_int), ("path", C.c_int),
+                ("maxQuerySize", C.c_uint32), ("laneWords", C.c_uint32), ("useGraphs", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("refused", C.c_uint64), ("completed", C.c_uint64),
+                ("batches", C.c_uint64), ("batchCandidatesMax", C.c_uint64), ("candidatesCompleted", C.c_uint64),
+                ("slots", C.c_uint32), ("maxBatchCandidates", C.c_uint32), ("maxBatchQueries", C.c_uint32),
+                ("maxBatchEntries", C.c_uint32)]
+
+
+class Server:
+    """Continuous-batching request loop over a resident reference."""
+
+    def __init__(self, ref, distance=0.2, slots=0, budget=0, max_batch_candidates=0, max_queued=0,
+                 window=WINDOW_ALIGNED, path=PATH_BATCHED, max_query_size=0, lane_words=0, graphs=True):
+        cfg = ServerConfig(budget, slots, max_batch_candidates, max_queued, distance, window, path, max_query_size,
+                           lane_words, int(graphs))
+        self.h = C.c_void_p()
+        check(lib.myersServerCreate(C.byref(self.h), ref.h, C.byref(cfg)), "myersServerCreate")
+
+    def submit(self, peq_entries, query_size, positions):
+        """Returns (status, ticket); status E_BUSY means the request was refused."""
+        peq_entries = np.ascontiguousarray(peq_entries)
+        pos = np.ascontiguousarray(positions, dtype=np.uint64)
+        t = C.c_uint64()
+        st = lib.myersServerSubmit(self.h, peq_entries.ctypes.data, query_size, pos.ctypes.data, len(pos),
+                                   C.byref(t))
+        return st, t.value
+
+    def wait(self, ticket, n, timeout_ms=60000):
+        out = np.empty(n, dtype=RES)
+        st = lib.myersServerWait(self.h, ticket, out.ctypes.data, timeout_ms)
+        return st, out
+
+    def poll(self, ticket, n):
+        out = np.empty(n, dtype=RES)
+        return lib.myersServerPoll(self.h, ticket, out.ctypes.data), out
+
+    def stats(self):
+        s = ServerStats()
+        check(lib.myersServerStats(self.h, C.byref(s)), "myersServerStats")
+        return {f: getattr(s, f) for f, _ in s._fields_}
+
+    def replay(self, peq, qinfo, cand_offset, positions, arrival_ns):
+        """Open-loop replay; returns (status, latency_ns per request, results, wall_ns)."""
+        n = len(qinfo)
+        lat = np.empty(n, dtype=np.uint64)
+        res = np.empty(int(cand_offset[-1]), dtype=RES)
+        wall = C.c_uint64()
+        peq, qinfo = np.ascontiguousarray(peq), np.ascontiguousarray(qinfo)
+        off = np.ascontiguousarray(cand_offset, dtype=np.uint32)
+        pos = np.ascontiguousarray(positions, dtype=np.uint64)
+        arr = np.ascontiguousarray(arrival_ns, dtype=np.uint64)
+        st = lib.myersServerReplay(self.h, peq.ctypes.data, qinfo.ctypes.data, off.ctypes.data, pos.ctypes.data, n,
+                                   arr.ctypes.data, lat.ctypes.data, res.ctypes.data, C.byref(wall))
+        return st, lat, res, wall.value
+
+    def close(self):
+        if self.h:
+            lib.myersServerDestroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ---------------------------------------------------------------------------
