@@ -192,13 +192,12 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
   if (lane_words > 0 && w > lane_words) {
     for (int mi = 0; mi < kNumMulti; ++mi) {
       const uint32_t W = (uint32_t)kMultiW[mi];
-      if (W < lane_words || (batched && W > (uint32_t)kBatchedMaxW)) continue;
+      if (W < lane_words || (batched && W > (uint32_t)kBatchedMaxMultiW)) continue;
       const uint32_t L = (w + W - 1) / W;
       if (L >= 2 && L <= 32) return Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};
     }
   }
-  const uint32_t single_max = batched ? (uint32_t)kBatchedMaxW : 32u;
-  if (w <= single_max) return Shape{(uint8_t)(w - 1), 1, (uint8_t)w, 0};
+  if (w <= 32) return Shape{(uint8_t)(w - 1), 1, (uint8_t)w, 0};
   double best = 1e300;
   Shape bs{0, 0, 0, 0};
   for (int mi = 0; mi < kNumMulti; ++mi) {
@@ -207,7 +206,7 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
     if (L < 2 || L > 32) continue;
     const double c = shape_cost(kNumSingle + mi, (int)L);
     // batched shapes that the persistent kernel cannot carry cost extra
-    const double pen = (batched && W > kBatchedMaxW) ? 4.0 : 1.0;
+    const double pen = (batched && W > kBatchedMaxMultiW) ? 4.0 : 1.0;
     if (c * pen < best) {
       best = c * pen;
       bs = Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};

@@ -35,8 +35,9 @@ constexpr int kNumSingle = 32;
 constexpr int kMultiW[] = {4, 6, 8, 10, 12, 16, 32};
 constexpr int kNumMulti = sizeof(kMultiW) / sizeof(kMultiW[0]);
 constexpr int kNumVariants = kNumSingle + kNumMulti;
-// The persistent kernel carries single W <= 16 and multi W <= 16.
-constexpr int kBatchedMaxW = 16;
+// The persistent kernel carries every single-lane shape and multi-lane
+// shapes up to 16 words per lane.
+constexpr int kBatchedMaxMultiW = 16;
 
 // A length bucket's launch shape: variant (kernel template), lanes per
 // candidate L and words per lane W. Buckets are indexed by the number of
@@ -94,7 +95,7 @@ struct DevInputs {
 
 inline int variant_W(int v) { return v < kNumSingle ? v + 1 : kMultiW[v - kNumSingle]; }
 inline bool variant_multi(int v) { return v >= kNumSingle; }
-inline bool batched_supports(int v) { return variant_W(v) <= kBatchedMaxW; }
+inline bool batched_supports(int v) { return !variant_multi(v) || variant_W(v) <= kBatchedMaxMultiW; }
 
 // ---- host launchers (myers_kernels.cu) ----
 

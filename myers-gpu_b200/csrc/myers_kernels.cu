@@ -70,25 +70,36 @@ __device__ __forceinline__ uint32_t qword(const uint32_t* __restrict__ peq, uint
                             : 0u;
 }
 
-// Shared-memory PEQ layout of one warp: [group g][base c][lane][4 words],
-// group g holding words 4g..4g+3 of a lane's W words. The eight lanes of one
-// LDS.128 phase always touch eight different 16-byte bank groups, whatever
-// bases they read, so the per-column loads are free of bank conflicts.
-constexpr int kLaneStride = 4;              // words between lanes
-constexpr int kBaseStride = 32 * 4;         // words between bases of a group
-constexpr int kGroupStride = 5 * 32 * 4;    // words between groups
+// Shared-memory PEQ of one warp. Candidates of the same read share one slot
+// (the candidates of a read are adjacent in a tile), so a warp stages one
+// copy per distinct read. Layout: [group g][base c][column][4 words], group g
+// holding words 4g..4g+3 of a lane's W words and column = slot * L + lane in
+// the segment. NCOL (the column count) is 1 mod 8, so the eight lanes of one
+// LDS.128 phase that read the same slot with different bases hit different
+// 16-byte bank groups.
+template <int W, bool MULTI>
+struct Layout {
+  static constexpr int GW = (W + 3) / 4;
+  // single-lane shapes: up to 32 slots (16 for W > 16, which halves the
+  // footprint of the widest shapes); multi-lane: one column per lane
+  static constexpr int SLOTS = MULTI ? 32 : (W > 16 ? 16 : 32);
+  static constexpr int NCOL = ((SLOTS + 7) / 8) * 8 + 1;
+  static constexpr int BASE = NCOL * 4;       // words between bases of a group
+  static constexpr int GROUP = 5 * NCOL * 4;  // words between groups
+  static constexpr int WORDS = GW * GROUP;    // per warp
+};
 
 // Stage lane l's W words (of a 32*LW-row top-aligned query) for all five
-// bases. `dst` = the warp's region + lane * kLaneStride.
-template <int W>
+// bases. `dst` = the warp's region + column * 4.
+template <int W, bool MULTI>
 __device__ __forceinline__ void stage_lane(uint32_t* __restrict__ dst, const uint32_t* __restrict__ peq,
                                            uint32_t pos_entry, uint32_t m, int LW, int l) {
-  constexpr int GW = (W + 3) / 4;
+  using Lay = Layout<W, MULTI>;
   const int nw = (int)((m + 31) >> 5);
   const int p = LW * 32 - (int)m;
   const int pw = p >> 5, ps = p & 31;
 #pragma unroll 1
-  for (int g = 0; g < GW; ++g) {
+  for (int g = 0; g < Lay::GW; ++g) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
       uint32_t v[4];
@@ -99,18 +110,18 @@ __device__ __forceinline__ void stage_lane(uint32_t* __restrict__ dst, const uin
         uint32_t lo = qword(peq, pos_entry, nw, c, a - 1);
         v[j] = ps ? __funnelshift_r(lo, hi, 32 - ps) : hi;
       }
-      *reinterpret_cast<uint4*>(dst + g * kGroupStride + c * kBaseStride) = make_uint4(v[0], v[1], v[2], v[3]);
+      *reinterpret_cast<uint4*>(dst + g * Lay::GROUP + c * Lay::BASE) = make_uint4(v[0], v[1], v[2], v[3]);
     }
   }
 }
 
 // The W Eq words of one base; `p` points at the lane's words of that base
 // in group 0.
-template <int W>
+template <int W, bool MULTI>
 __device__ __forceinline__ void load_eq(const uint32_t* __restrict__ p, uint32_t (&eq)[W]) {
 #pragma unroll
   for (int g = 0; g < (W + 3) / 4; ++g) {
-    const uint32_t* q = p + g * kGroupStride;
+    const uint32_t* q = p + g * Layout<W, MULTI>::GROUP;
     if (4 * g + 4 <= W) {
       uint4 v = *reinterpret_cast<const uint4*>(q);
       eq[4 * g] = v.x;
@@ -207,9 +218,9 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
                                               uint32_t colbase, uint32_t n, Mul k) {
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const uint32_t off = ((t >> (4 * u)) & 7u) << 9;  // base * kBaseStride * 4 bytes
+    const uint32_t off = ((t >> (4 * u)) & 7u) * (uint32_t)(Layout<W, false>::BASE * 4);
     uint32_t eq[W];
-    load_eq<W>(reinterpret_cast<const uint32_t*>(slot + off), eq);
+    load_eq<W, false>(reinterpret_cast<const uint32_t*>(slot + off), eq);
     uint32_t tp, tm;
     myers_column<W, false>(eq, Pv, Mv, 0u, 0u, tp, tm, k);
     sc += (tp >> 31) << 16;
@@ -221,11 +232,13 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
 
 struct CandSetup {
   uint32_t id;
+  uint32_t query;
   unsigned long long pos;
   uint32_t m;
   uint32_t pos_entry;
   uint32_t n;     // columns
-  bool has;       // the slot holds a candidate
+  bool has;       // the segment holds a candidate
+  bool qok;       // ... whose query can be staged (valid indices, 0 < m <= rows)
   bool work;      // ... that needs the DP
 };
 
@@ -250,6 +263,8 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
   c.m = 0;
   c.pos_entry = 0;
   c.n = 0;
+  c.query = 0;
+  c.qok = false;
   c.work = false;
   if (c.has) {
     c.id = ids ? __ldg(ids + first + seg) : first + (uint32_t)seg;
@@ -258,6 +273,7 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
     uint32_t bad = 0u;
     if (cd.query < in.num_queries) q = __ldg(in.qinfo + cd.query);
     bad = check_query(in, cd.query, q);
+    c.query = cd.query;
     c.pos = cd.position;
     c.pos_entry = q.x;
     c.m = q.y;
@@ -265,6 +281,7 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
     const bool valid = bad == 0u && c.pos < in.ref_size && (in.ref_size - c.pos) > (unsigned long long)wb;
     c.n = in.exact ? wb : 8u * d_window_words(wb);
     const bool fits = c.m <= (uint32_t)rows && c.n <= kMaxColumns;
+    c.qok = bad == 0u && c.m > 0 && c.m <= (uint32_t)rows;
     c.work = valid && c.m > 0 && fits;
     if (!c.work && l == 0) {
       in.results[c.id] = (valid && c.m == 0) ? make_uint2(0u, 0u) : make_uint2(0u, kNoResult);
@@ -278,91 +295,112 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
 template <int W, bool MULTI>
 __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
                                              uint32_t cnt, int L, uint32_t* __restrict__ wsmem, int lane) {
+  using Lay = Layout<W, MULTI>;
   const int Lr = MULTI ? L : 1;
   const int nseg = MULTI ? 32 / L : 32;
   const int seg = MULTI ? lane / L : lane;
   const int l = MULTI ? lane - seg * L : 0;
   const int LW = Lr * W;
   const int rows = 32 * LW;
-  uint32_t* lane_part = wsmem + lane * kLaneStride;
 
   const CandSetup c = setup_candidate(in, ids, first, cnt, seg, nseg, l, rows);
-  if (c.work) stage_lane<W>(lane_part, in.peq, c.pos_entry, c.m, LW, l);
-  __syncwarp();
+
+  // One slot per run of segments with the same read: a run starts where the
+  // read differs from the previous segment's.
+  const uint32_t qkey = c.has ? c.query : 0xFFFFFFFFu;
+  const uint32_t qprev = __shfl_up_sync(FULL_MASK, qkey, Lr);
+  const bool starts = c.has && (seg == 0 || qprev != qkey);
+  const unsigned run_starts = __ballot_sync(FULL_MASK, starts && l == 0);
+  const int my_bit = seg * Lr;
+  const int run = __popc(run_starts & (my_bit >= 31 ? FULL_MASK : ((2u << my_bit) - 1u))) - 1;
+  const int distinct = __popc(run_starts);
+  // more distinct reads than slots (single-lane wide shapes only): rounds
+  const int rounds = (distinct + Lay::SLOTS / Lr - 1) / (Lay::SLOTS / Lr);
 
   const uint32_t p = (uint32_t)rows - c.m;
-  uint32_t Pv[W], Mv[W];
-#pragma unroll
-  for (int j = 0; j < W; ++j) {
-    Pv[j] = 0xFFFFFFFFu;
-    Mv[j] = 0u;
-  }
-  uint32_t sc = (uint32_t)rows << 16;  // score + p = rows at column -1
-  uint32_t kmin = sc;                  // (score, column) = (m, 0) before any column
   const long long q0 = (long long)(in.exact ? c.pos : (c.pos & ~7ull)) - l;
   const long long b0 = q0 >> 3;
   const uint32_t sh = 4u * (uint32_t)(q0 & 7);
-  const char* slot = reinterpret_cast<const char*>(lane_part);
   const Mul k{in.one, in.two};
 
-  if constexpr (!MULTI) {
-    if (c.work) {
+  for (int r = 0; r < rounds; ++r) {
+    const int slot = run - r * (Lay::SLOTS / Lr);
+    const bool in_round = c.has && slot >= 0 && slot < Lay::SLOTS / Lr;
+    const int col = in_round ? slot * Lr + l : l;
+    uint32_t* lane_part = wsmem + col * 4;
+    if (in_round && starts && c.qok) stage_lane<W, MULTI>(lane_part, in.peq, c.pos_entry, c.m, LW, l);
+    __syncwarp();
+    const bool work = c.work && in_round;
+    const char* slotp = reinterpret_cast<const char*>(lane_part);
+
+    uint32_t Pv[W], Mv[W];
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      Pv[j] = 0xFFFFFFFFu;
+      Mv[j] = 0u;
+    }
+    uint32_t sc = (uint32_t)rows << 16;  // score + p = rows at column -1
+    uint32_t kmin = sc;                  // (score, column) = (m, 0) before any column
+
+    if constexpr (!MULTI) {
+      if (work) {
+        uint32_t lo = ref_load(in.ref, b0, in.ref_words);
+        uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
+        const uint32_t nfull = c.n >> 3;
+        uint32_t i = 0;
+        for (; i < nfull; ++i) {
+          const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+          lo = hi;
+          hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+          block8_single<W, false>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
+        }
+        if (c.n & 7u) {
+          const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+          block8_single<W, true>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
+        }
+        in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
+      }
+    } else {
+      uint32_t steps = work ? c.n + (uint32_t)L - 1u : 0u;
+      steps = __reduce_max_sync(FULL_MASK, steps);
+      const uint32_t nblk = (steps + 7u) >> 3;
       uint32_t lo = ref_load(in.ref, b0, in.ref_words);
       uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
-      const uint32_t nfull = c.n >> 3;
-      uint32_t i = 0;
-      for (; i < nfull; ++i) {
+      uint32_t outP = 0u, outM = 0u;
+      const bool seg_start = (l == 0);
+      for (uint32_t i = 0; i < nblk; ++i) {
         const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
         lo = hi;
         hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
-        block8_single<W, false>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n, k);
-      }
-      if (c.n & 7u) {
-        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
-        block8_single<W, true>(t, slot, Pv, Mv, sc, kmin, 8u * i, c.n, k);
-      }
-      in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
-    }
-  } else {
-    uint32_t steps = c.work ? c.n + (uint32_t)L - 1u : 0u;
-    steps = __reduce_max_sync(FULL_MASK, steps);
-    const uint32_t nblk = (steps + 7u) >> 3;
-    uint32_t lo = ref_load(in.ref, b0, in.ref_words);
-    uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
-    uint32_t outP = 0u, outM = 0u;
-    const bool seg_start = (l == 0);
-    for (uint32_t i = 0; i < nblk; ++i) {
-      const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
-      lo = hi;
-      hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const uint32_t off = ((t >> (4 * u)) & 7u) << 9;
-        uint32_t eq[W];
-        load_eq<W>(reinterpret_cast<const uint32_t*>(slot + off), eq);
-        uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1);
-        uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1);
-        if (seg_start) {
-          inP = 0u;
-          inM = 0u;
-        }
-        const uint32_t j = 8u * i + (uint32_t)u - (uint32_t)l;  // wraps when negative
-        if (c.work && j < c.n) {
-          myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM, k);
-          sc += (outP >> 31) << 16;
-          sc -= (outM >> 31) << 16;
-          kmin = min(kmin, sc + j);
+        for (int u = 0; u < 8; ++u) {
+          const uint32_t off = ((t >> (4 * u)) & 7u) * (uint32_t)(Lay::BASE * 4);
+          uint32_t eq[W];
+          load_eq<W, true>(reinterpret_cast<const uint32_t*>(slotp + off), eq);
+          uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1);
+          uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1);
+          if (seg_start) {
+            inP = 0u;
+            inM = 0u;
+          }
+          const uint32_t j = 8u * i + (uint32_t)u - (uint32_t)l;  // wraps when negative
+          if (work && j < c.n) {
+            myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM, k);
+            sc += (outP >> 31) << 16;
+            sc -= (outM >> 31) << 16;
+            kmin = min(kmin, sc + j);
+          }
         }
       }
+      if (work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
     }
-    if (c.work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
+    __syncwarp();
   }
-  __syncwarp();
 }
 
-template <int W>
+template <int W, bool MULTI>
 __host__ __device__ constexpr uint32_t warp_words() {
-  return (uint32_t)(((W + 3) / 4) * kGroupStride);
+  return (uint32_t)Layout<W, MULTI>::WORDS;
 }
 
 // Plain launch: one shape over a contiguous range of (sorted) candidates,
@@ -378,7 +416,7 @@ __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __r
     count = st->count[cfg];
   }
   const int nseg = MULTI ? 32 / L : 32;
-  uint32_t* wsmem = smem + wib * warp_words<W>();
+  uint32_t* wsmem = smem + wib * warp_words<W, MULTI>();
   const uint32_t tiles = (count + nseg - 1) / nseg;
   const uint32_t wpb = blockDim.x >> 5;
   for (uint32_t t = blockIdx.x * wpb + wib; t < tiles; t += gridDim.x * wpb) {
@@ -467,15 +505,18 @@ __global__ void k_scatter(uint32_t n, const uint8_t* __restrict__ cfg_of_cand, B
 
 // ---- the persistent batched kernel ----
 
-constexpr uint32_t kBatchedWarpWords = warp_words<kBatchedMaxW>();  // the largest batched shape
+constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
+// the largest batched shape's footprint
+constexpr uint32_t kBatchedWarpWords =
+    cmax(cmax(warp_words<32, false>(), warp_words<16, false>()), warp_words<kBatchedMaxMultiW, true>());
 
 template <int V>
 __device__ __forceinline__ void dispatch_one(const DevInputs& in, const uint32_t* ids, uint32_t f, uint32_t cnt,
                                              int L, uint32_t* wsmem, int lane) {
   if constexpr (V < kNumSingle) {
-    if constexpr (V + 1 <= kBatchedMaxW) process_tile<V + 1, false>(in, ids, f, cnt, L, wsmem, lane);
+    process_tile<V + 1, false>(in, ids, f, cnt, L, wsmem, lane);
   } else {
-    if constexpr (kMultiW[V - kNumSingle] <= kBatchedMaxW)
+    if constexpr (kMultiW[V - kNumSingle] <= kBatchedMaxMultiW)
       process_tile<kMultiW[V - kNumSingle], true>(in, ids, f, cnt, L, wsmem, lane);
   }
 }
@@ -571,7 +612,9 @@ static const auto kPlainTable = make_plain_table(std::make_integer_sequence<int,
 
 uint32_t warp_smem_bytes(int v, int) {
   const int W = variant_W(v);
-  return (uint32_t)(((W + 3) / 4) * kGroupStride * 4);
+  const int slots = variant_multi(v) ? 32 : (W > 16 ? 16 : 32);
+  const int ncol = ((slots + 7) / 8) * 8 + 1;
+  return (uint32_t)(((W + 3) / 4) * 5 * ncol * 4 * 4);
 }
 
 static int blocks_per_sm(const void* fn, int threads, size_t smem) {
