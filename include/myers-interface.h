@@ -347,6 +347,13 @@ int myersShapeOf(int path, uint32_t querySize, int *variant, int *L, int *W);
  * (ceil(size/32)); variant -1 restores the built-in choice. */
 int myersSetShapeOverride(int path, uint32_t words, int variant, int L);
 
+/* Shapes come, in this order, from myersSetShapeOverride, the serving loop's
+ * latency policy (laneWords), the autotuner's cache -- autotune_b200.json next
+ * to the library, written by myers-gpu_b200/autotune.py (MYERS_AUTOTUNE names
+ * another file, MYERS_AUTOTUNE=0 ignores it) -- and a built-in cost model.
+ * Returns how many word counts the loaded cache covers for the path. */
+int myersTunedShapes(int path);
+
 /* Integer-ALU throughput probe on the current device: 3-input logic ops per
  * second of a device-filling launch (the roofline denominator). */
 int myersProbeIntPeak(double *opsPerSecond, int iters);

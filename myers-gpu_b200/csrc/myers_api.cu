@@ -20,8 +20,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
+#include <dlfcn.h>
 #include <cuda_runtime.h>
 
 #include "../../include/myers-interface.h"
@@ -178,12 +180,66 @@ struct Override {
 };
 static std::mutex g_override_mu;
 static Override g_override[2][kMaxWords + 1];
+static Override g_tuned[2][kMaxWords + 1];  // from the autotuner's cache file
+
+// Load the autotuner's cache: `autotune_b200.json` next to this library (or
+// the file named by MYERS_AUTOTUNE; MYERS_AUTOTUNE=0 disables it). Format:
+// {"plain": {"<words>": [variant, L], ...}, "batched": {...}, ...}; entries
+// that name a shape the path cannot run are ignored.
+static void load_tuned_once() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    std::string path;
+    const char* env = getenv("MYERS_AUTOTUNE");
+    if (env && strcmp(env, "0") == 0) return;
+    if (env && *env) {
+      path = env;
+    } else {
+      Dl_info info;
+      if (dladdr((void*)&load_tuned_once, &info) == 0 || info.dli_fname == nullptr) return;
+      path = info.dli_fname;
+      const size_t slash = path.rfind('/');
+      path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/autotune_b200.json";
+    }
+    FILE* fp = fopen(path.c_str(), "rb");
+    if (fp == nullptr) return;
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), fp)) > 0) text.append(buf, n);
+    fclose(fp);
+    std::lock_guard<std::mutex> lk(g_override_mu);
+    for (int path_id = 0; path_id < 2; ++path_id) {
+      const char* key = path_id == 0 ? "\"plain\"" : "\"batched\"";
+      size_t at = text.find(key);
+      if (at == std::string::npos) continue;
+      at = text.find('{', at);
+      const size_t end = text.find('}', at);
+      if (at == std::string::npos || end == std::string::npos) continue;
+      const char* p = text.c_str() + at;
+      const char* e = text.c_str() + end;
+      while (p < e) {
+        unsigned w = 0;
+        int v = -1, L = 0, used = 0;
+        if (sscanf(p, " \"%u\" : [ %d , %d ]%n", &w, &v, &L, &used) == 3 && used > 0) {
+          if (w >= 1 && w <= kMaxWords && v >= 0 && v < kNumVariants && L >= 1 && L <= 32 &&
+              (uint32_t)(variant_W(v) * (variant_multi(v) ? L : 1)) >= w && (path_id == 0 || batched_supports(v)))
+            g_tuned[path_id][w] = Override{true, (uint8_t)v, (uint8_t)(variant_multi(v) ? L : 1)};
+          p += used;
+        } else {
+          ++p;
+        }
+      }
+    }
+  });
+}
 
 // lane_words > 0 asks for latency-oriented shapes: a query of more than
 // lane_words words is spread over ceil(words / W) lanes, W the smallest
 // multi-lane width >= lane_words (shorter per-candidate time, a few percent
 // more instructions).
 static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
+  load_tuned_once();
   {
     std::lock_guard<std::mutex> lk(g_override_mu);
     const Override& o = g_override[batched ? 1 : 0][w];
@@ -196,6 +252,11 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
       const uint32_t L = (w + W - 1) / W;
       if (L >= 2 && L <= 32) return Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};
     }
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_override_mu);
+    const Override& o = g_tuned[batched ? 1 : 0][w];
+    if (o.set) return Shape{o.variant, o.L, (uint8_t)variant_W(o.variant), 0};
   }
   if (w <= 32) return Shape{(uint8_t)(w - 1), 1, (uint8_t)w, 0};
   double best = 1e300;
@@ -455,6 +516,16 @@ extern "C" int myersShapeOf(int path, uint32_t querySize, int* variant, int* L, 
   *L = s.L;
   *W = s.W;
   return MYERS_SUCCESS;
+}
+
+// Word counts with an autotuned shape for the path (0 if no cache was loaded).
+extern "C" int myersTunedShapes(int path) {
+  if (path != MYERS_PATH_PLAIN && path != MYERS_PATH_BATCHED) return -1;
+  load_tuned_once();
+  std::lock_guard<std::mutex> lk(g_override_mu);
+  int n = 0;
+  for (uint32_t w = 1; w <= kMaxWords; ++w) n += g_tuned[path][w].set;
+  return n;
 }
 
 extern "C" int myersNumVariants(void) { return kNumVariants; }

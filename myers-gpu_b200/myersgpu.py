@@ -101,6 +101,7 @@ _sig("myersVariantWords", _I32, _I32)
 _sig("myersVariantIsMulti", _I32, _I32)
 _sig("myersShapeOf", _I32, _I32, _U32, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32))
 _sig("myersSetShapeOverride", _I32, _I32, _U32, _I32, _I32)
+_sig("myersTunedShapes", _I32, _I32)
 _sig("myersProbeIntPeak", _I32, C.POINTER(C.c_double), _I32)
 
 # Every symbol the C header declares (the CPU tests check the exports).
@@ -112,7 +113,7 @@ EXPORTED = (
     "myersReferenceLoad myersReferenceDestroy myersReferenceSize myersContextCreate myersContextDestroy "
     "myersVerifyAsync myersVerifyRangeAsync myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
     "myersBufferLastLaunches myersNumVariants myersVariantWords myersVariantIsMulti myersShapeOf "
-    "myersSetShapeOverride myersProbeIntPeak myersServerCreate myersServerSubmit myersServerPoll myersServerWait "
+    "myersSetShapeOverride myersTunedShapes myersProbeIntPeak myersServerCreate myersServerSubmit myersServerPoll myersServerWait "
     "myersServerStats myersServerDestroy myersServerReplay"
 ).split()
 

@@ -41,19 +41,38 @@ def test_error_strings(mg):
 
 
 def test_shape_choice(mg):
-    for m in (1, 31, 32, 33, 100, 1000, 1024):
-        v, L, W = mg.shape_of(m, mg.PATH_PLAIN)
-        assert L == 1 and W == (m + 31) // 32 and v == W - 1
-    for m in (1025, 3000, 10000, 32768):
-        v, L, W = mg.shape_of(m, mg.PATH_PLAIN)
-        assert L > 1 and L * W * 32 >= m and L <= 32
-    for m in (100, 512, 513, 1000, 10000, 16384):
-        v, L, W = mg.shape_of(m, mg.PATH_BATCHED)
-        assert L * W * 32 >= m and W <= 16
+    """Whatever picks the shape (autotuner cache or cost model), it must hold
+    the query, and the batched path must only pick shapes its persistent
+    kernel carries (or, beyond 16384 bases, multi-lane shapes it launches
+    plainly)."""
+    for path in (mg.PATH_PLAIN, mg.PATH_BATCHED):
+        for m in (1, 31, 32, 33, 100, 513, 1000, 1024, 1025, 3000, 10000, 16384, 20000, 32768):
+            v, L, W = mg.shape_of(m, path)
+            multi = bool(mg.lib.myersVariantIsMulti(v))
+            assert W == mg.lib.myersVariantWords(v)
+            assert 1 <= L <= 32 and L * W * 32 >= m
+            assert multi or L == 1
+            if path == mg.PATH_BATCHED and multi and m <= 16384:
+                assert W <= 16
     with pytest.raises(mg.MyersError):
         mg.shape_of(0)
     with pytest.raises(mg.MyersError):
         mg.shape_of(mg.MAX_QUERY_BASES + 1)
+
+
+def test_cost_model_without_cache():
+    """With the autotuner's cache disabled, the built-in cost model gives one
+    candidate per lane up to 1024 bases."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, 'myers-gpu_b200'); import myersgpu as mg;"
+            "assert mg.lib.myersTunedShapes(0) == 0;"
+            "print([mg.shape_of(m, p)[1:] for p in (0, 1) for m in (1, 100, 1000, 1024, 1025, 10000)])")
+    env = dict(__import__('os').environ, MYERS_AUTOTUNE="0")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, check=True)
+    shapes = eval(out.stdout)
+    assert shapes[:4] == [(1, 1), (1, 4), (1, 32), (1, 32)] and shapes[6:10] == [(1, 1), (1, 4), (1, 32), (1, 32)]
+    assert shapes[4][0] > 1 and shapes[5][0] > 1
 
 
 def test_shape_override(mg):
