@@ -140,6 +140,17 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def reduce_over_ranks(dist, elapsed_s, n_cands, cells, device):
+    """Whole-job numbers of a replicas run: the slowest rank's timed seconds,
+    and the candidates and DP cells all ranks verified."""
+    import torch
+    t = torch.tensor([elapsed_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot = torch.tensor([float(n_cands), float(cells)], dtype=torch.float64, device=device)
+    dist.all_reduce(tot)
+    return float(t.item()), float(tot[0].item()), float(tot[1].item())
+
+
 def make_inputs(mg, k, scale, seed_offset, num_reads=None):
     s = mg.workload_spec(k, scale=scale)
     s.seed += 7919 * seed_offset
@@ -281,12 +292,7 @@ def run_ours(args):
     step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     elapsed = sum(step_ms) / 1e3
     if dist is not None:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-        tot = torch.tensor([float(n_cands), float(cells.sum())], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tot)
-        all_cands, all_cells = float(tot[0].item()), float(tot[1].item())
+        elapsed, all_cands, all_cells = reduce_over_ranks(dist, elapsed, n_cands, cells.sum(), "cuda")
     else:
         all_cands, all_cells = float(n_cands), float(cells.sum())
     value = all_cands * args.steps / elapsed

@@ -252,6 +252,23 @@ int myersVerifyNoAllocAsync(const uint32_t *d_refWords, uint64_t refWords, uint6
                             uint32_t minQuerySize, uint32_t maxQuerySize,
                             resEntry_t *d_results, void *stream);
 
+/* Build PEQ entries from ASCII reads on the device (the packing of
+ * src-api/genCandidate-reorder.c:258-317): read r is
+ * d_ascii[d_offsets[r] .. d_offsets[r] + d_qinfo[r].size) (A/C/G/T either
+ * case, anything else N); its ceil(size/128) entries are written at
+ * d_peq + d_qinfo[r].posEntry. d_ascii holds asciiBytes bytes, d_offsets
+ * numReads + 1 entries; reads whose bytes or entries fall outside the
+ * buffers are skipped and raise context flag 4. */
+int myersPackPEQAsync(myersContext_t *ctx, const uint8_t *d_ascii, uint64_t asciiBytes,
+                      const uint64_t *d_offsets, const qryInfo_t *d_qinfo, uint32_t numReads,
+                      qryEntry_t *d_peq, uint32_t numPEQEntries, void *stream);
+
+/* Pack ASCII bases into reference words on the device (the packing of
+ * src-api/genReference-4bits.c:43-72): numWords words, 8 bases each, base i
+ * in bits 4*(i%8) of word i/8; bases at or past numBases are N. */
+int myersPackReferenceAsync(const uint8_t *d_ascii, uint64_t numBases, uint32_t *d_words,
+                            uint64_t numWords, void *stream);
+
 /* Kernel launches the last myersVerify*Async on this context enqueued. */
 uint32_t myersContextLastLaunches(const myersContext_t *ctx);
 

@@ -485,6 +485,35 @@ extern "C" int myersContextFlags(myersContext_t* ctx, uint32_t* flags, int clear
   return MYERS_SUCCESS;
 }
 
+// PEQ entries from ASCII reads on the device (genCandidate-reorder.c:258-317
+// as a kernel): read r is ascii[offsets[r] .. offsets[r] + qinfo[r].size),
+// its entries go to d_peq + qinfo[r].posEntry. Reads whose entries or bytes
+// fall outside the buffers are skipped and raise flag 4 on the context.
+extern "C" int myersPackPEQAsync(myersContext_t* ctx, const uint8_t* d_ascii, uint64_t asciiBytes,
+                                 const uint64_t* d_offsets, const qryInfo_t* d_qinfo, uint32_t numReads,
+                                 qryEntry_t* d_peq, uint32_t numPEQEntries, void* stream) {
+  if (ctx == nullptr || (numReads > 0 && (d_ascii == nullptr || d_offsets == nullptr || d_qinfo == nullptr ||
+                                           d_peq == nullptr)))
+    return MYERS_E_INVALID_ARGUMENT;
+  CU(launch_pack_peq(d_ascii, asciiBytes, reinterpret_cast<const unsigned long long*>(d_offsets),
+                     reinterpret_cast<const uint2*>(d_qinfo), numReads, reinterpret_cast<uint32_t*>(d_peq),
+                     numPEQEntries, ctx->d_flags, (cudaStream_t)stream, ctx->num_sms));
+  return MYERS_SUCCESS;
+}
+
+// Packed reference words from ASCII bases on the device
+// (genReference-4bits.c:43-72 as a kernel): numWords words, bases at or past
+// numBases are N.
+extern "C" int myersPackReferenceAsync(const uint8_t* d_ascii, uint64_t numBases, uint32_t* d_words,
+                                       uint64_t numWords, void* stream) {
+  if (numWords > 0 && (d_ascii == nullptr || d_words == nullptr)) return MYERS_E_INVALID_ARGUMENT;
+  int dev = 0, sms = 0;
+  CU(cudaGetDevice(&dev));
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CU(launch_pack_reference(d_ascii, numBases, d_words, numWords, (cudaStream_t)stream, sms));
+  return MYERS_SUCCESS;
+}
+
 // Autotuner hook: force the shape of one word count (variant, L); variant
 // -1 clears the override.
 extern "C" int myersSetShapeOverride(int path, uint32_t words, int variant, int L) {

@@ -119,6 +119,13 @@ cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const Pla
 // Bytes of shared memory one warp needs for a shape.
 uint32_t warp_smem_bytes(int v, int L);
 
+// Packers (ASCII -> PEQ entries; ASCII -> packed reference words).
+cudaError_t launch_pack_peq(const uint8_t* ascii, unsigned long long ascii_bytes, const unsigned long long* offsets,
+                            const uint2* qinfo, uint32_t num_reads, uint32_t* peq, uint32_t num_entries,
+                            uint32_t* flags, cudaStream_t s, int num_sms);
+cudaError_t launch_pack_reference(const uint8_t* ascii, unsigned long long n, uint32_t* words,
+                                  unsigned long long nwords, cudaStream_t s, int num_sms);
+
 // Integer-ALU peak probe: `iters` rounds of independent 3-input logic ops.
 cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iters, cudaStream_t s);
 

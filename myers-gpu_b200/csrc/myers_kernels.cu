@@ -678,3 +678,80 @@ cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iter
 }
 
 }  // namespace myers
+
+// ---- packers on the device ----
+
+namespace myers {
+
+// ASCII base -> code: A0 C1 G2 T3 (either case), anything else 4
+// (src-api/genReference-4bits.c:21-40, genCandidate-reorder.c:237-256).
+__device__ __forceinline__ uint32_t ascii_code(uint32_t b) {
+  const uint32_t u = b & 0xDFu;  // upper case
+  return u == 'A' ? 0u : u == 'C' ? 1u : u == 'G' ? 2u : u == 'T' ? 3u : 4u;
+}
+
+// One thread per 32-base word of a read: the five 32-bit bitmaps of that
+// word. Bits past the read's end are 0 (src-api/genCandidate-reorder.c:258-317).
+__global__ void k_pack_peq(const uint8_t* __restrict__ ascii, unsigned long long ascii_bytes,
+                           const unsigned long long* __restrict__ offsets, const uint2* __restrict__ qinfo,
+                           uint32_t num_reads, uint32_t* __restrict__ peq, uint32_t num_entries,
+                           uint32_t* __restrict__ flags) {
+  const uint32_t stride = gridDim.x * (blockDim.x / 32);
+  const int lane = threadIdx.x & 31;
+  for (uint32_t r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); r < num_reads; r += stride) {
+    const uint2 q = qinfo[r];
+    const unsigned long long o = offsets[r];
+    const uint32_t m = q.y;
+    const uint32_t nwords = ((m + 127) / 128) * 4;  // whole entries, padding words zeroed
+    const unsigned long long o1 = offsets[r + 1];
+    if ((unsigned long long)q.x + nwords / 4 > num_entries || o1 < o || o1 - o < m || o1 > ascii_bytes) {
+      if (lane == 0) atomicOr(flags, kFlagBadEntry);
+      continue;
+    }
+    for (uint32_t w = lane; w < nwords; w += 32) {
+      uint32_t bm[5] = {0u, 0u, 0u, 0u, 0u};
+      const uint32_t b0 = w * 32;
+      for (uint32_t i = 0; i < 32 && b0 + i < m; ++i) bm[ascii_code(ascii[o + b0 + i])] |= 1u << i;
+      uint32_t* e = peq + (size_t)(q.x + w / 4) * 20;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) e[c * 4 + (w & 3)] = bm[c];
+    }
+  }
+}
+
+// One thread per packed word: eight bases, base i in bits 4*(i%8); bases at
+// or past n are N (src-api/genReference-4bits.c:43-72).
+__global__ void k_pack_reference(const uint8_t* __restrict__ ascii, unsigned long long n, uint32_t* __restrict__ words,
+                                 unsigned long long nwords) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long w = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += stride) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const unsigned long long i = w * 8 + k;
+      v |= (i < n ? ascii_code(ascii[i]) : 4u) << (4 * k);
+    }
+    words[w] = v;
+  }
+}
+
+cudaError_t launch_pack_peq(const uint8_t* ascii, unsigned long long ascii_bytes, const unsigned long long* offsets,
+                            const uint2* qinfo, uint32_t num_reads, uint32_t* peq, uint32_t num_entries,
+                            uint32_t* flags, cudaStream_t s, int num_sms) {
+  if (num_reads == 0) return cudaSuccess;
+  uint32_t grid = (num_reads + 7) / 8;
+  if (grid > (uint32_t)num_sms * 16) grid = (uint32_t)num_sms * 16;
+  k_pack_peq<<<grid, 256, 0, s>>>(ascii, ascii_bytes, offsets, qinfo, num_reads, peq, num_entries, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_reference(const uint8_t* ascii, unsigned long long n, uint32_t* words,
+                                  unsigned long long nwords, cudaStream_t s, int num_sms) {
+  if (nwords == 0) return cudaSuccess;
+  unsigned long long grid = (nwords + 255) / 256;
+  if (grid > (unsigned long long)num_sms * 32) grid = (unsigned long long)num_sms * 32;
+  k_pack_reference<<<(unsigned)grid, 256, 0, s>>>(ascii, n, words, nwords);
+  return cudaGetLastError();
+}
+
+}  // namespace myers

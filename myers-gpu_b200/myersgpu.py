@@ -88,6 +88,8 @@ _sig("myersVerifyAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _
 _sig("myersVerifyRangeAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _U32, _U32, _P, _P)
 _sig("myersVerifyNoAllocAsync", _I32, _P, _U64, _U64, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _U32, _U32, _P, _P)
 _sig("myersContextLastLaunches", _U32, _P)
+_sig("myersPackPEQAsync", _I32, _P, _P, _U64, _P, _P, _U32, _P, _U32, _P)
+_sig("myersPackReferenceAsync", _I32, _P, _U64, _P, _U64, _P)
 _sig("myersServerCreate", _I32, _PP, _P, _P)
 _sig("myersServerSubmit", _I32, _P, _P, _U32, _P, _U32, C.POINTER(_U64))
 _sig("myersServerPoll", _I32, _P, _U64, _P)
@@ -112,6 +114,7 @@ EXPORTED = (
     "myersSetKernelPath myersSetMemoryBudget myersGetDevice myersGetLastStatus myersReferenceCreate "
     "myersReferenceLoad myersReferenceDestroy myersReferenceSize myersContextCreate myersContextDestroy "
     "myersVerifyAsync myersVerifyRangeAsync myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
+    "myersPackPEQAsync myersPackReferenceAsync "
     "myersBufferLastLaunches myersNumVariants myersVariantWords myersVariantIsMulti myersShapeOf "
     "myersSetShapeOverride myersTunedShapes myersProbeIntPeak myersServerCreate myersServerSubmit myersServerPoll myersServerWait "
     "myersServerStats myersServerDestroy myersServerReplay"
