@@ -440,6 +440,26 @@ def run_serving(args):
     torch.cuda.synchronize()
     batched_cps = n_cands * args.steps / (a.elapsed_time(b) / 1e3)
     batched_res = d_res.cpu().numpy().view(mg.RES)
+    # the same, with the shapes the server picks (latency shapes), to split the
+    # serving gap into shape cost and serving-loop cost
+    same_cps = None
+    if args.lane_words > 0:
+        widths = sorted(W for v, W, multi in mg.variants() if multi and W <= 16)
+        Wl = min([W for W in widths if W >= args.lane_words] or [widths[-1]])
+        v_l = [v for v, W, multi in mg.variants() if multi and W == Wl][0]
+        words = range(args.lane_words + 1, 33)
+        for wd in words:
+            mg.set_shape_override(mg.PATH_BATCHED, wd, v_l, -(-wd // Wl))
+        for _ in range(2):
+            step()
+        a.record(st)
+        for _ in range(args.steps):
+            step()
+        b.record(st)
+        torch.cuda.synchronize()
+        same_cps = n_cands * args.steps / (a.elapsed_time(b) / 1e3)
+        for wd in words:
+            mg.set_shape_override(mg.PATH_BATCHED, wd, -1)
     ctx.close()
     del d_peq, d_qi, d_c, d_res
 
@@ -477,6 +497,8 @@ def run_serving(args):
                                   "graphs": not args.no_graphs}},
             "serving": {"sweep": sweep, "best": best, "batched_cand_s": batched_cps,
                         "served_frac_of_batched": value / batched_cps,
+                        "batched_same_shapes_cand_s": same_cps,
+                        "served_frac_of_batched_same_shapes": (value / same_cps) if same_cps else None,
                         "results_equal_to_batched": same, "batches": stats["batches"],
                         "largest_batch_candidates": stats["batchCandidatesMax"]},
             "e2e": {"value": value, "unit": "candidates/s",

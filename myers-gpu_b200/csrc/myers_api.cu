@@ -398,8 +398,7 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
   in.ref_size = ref->size;
   in.ref_words = ref->words + kRefPadWords;
   in.flags = ctx->d_flags;
-  in.one = 1u;
-  in.two = 2u;
+  set_multipliers(in);
   ctx->last_launches = 0;
   if (in.num_cands == 0) return MYERS_SUCCESS;
   if (in.num_cands > ctx->capacity) return MYERS_E_CAPACITY;
@@ -948,8 +947,7 @@ extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refW
   in.num_entries = numPEQEntries;
   in.distance = distance;
   in.exact = windowMode == MYERS_WINDOW_EXACT;
-  in.one = 1u;
-  in.two = 2u;
+  set_multipliers(in);
   cudaStream_t s = (cudaStream_t)stream;
   // the array keeps the previous call's contents: the bucket table (counts,
   // cursors, work queue) and the flags must start at zero

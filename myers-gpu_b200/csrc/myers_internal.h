@@ -89,9 +89,20 @@ struct DevInputs {
   uint32_t num_entries;
   float distance;
   int exact;
-  uint32_t one;                  // 1 and 2, set by the host: multipliers the
-  uint32_t two;                  // compiler cannot fold (see myers_kernels.cu)
+  // Multipliers the compiler cannot fold (set by set_multipliers): they keep
+  // the per-column bookkeeping on the FMA pipe (see myers_kernels.cu).
+  uint32_t one, two, k16, mk16, p28, kb33, kb17;
 };
+
+inline void set_multipliers(DevInputs& in) {
+  in.one = 1u;
+  in.two = 2u;
+  in.k16 = 1u << 16;
+  in.mk16 = 0xFFFF0000u;
+  in.p28 = 1u << 28;
+  in.kb33 = 33u * 4u * 4u;  // bytes between the bases of a PEQ group, 33 columns
+  in.kb17 = 17u * 4u * 4u;  // ... 17 columns
+}
 
 inline int variant_W(int v) { return v < kNumSingle ? v + 1 : kMultiW[v - kNumSingle]; }
 inline bool variant_multi(int v) { return v >= kNumSingle; }

@@ -143,11 +143,37 @@ __device__ __forceinline__ void load_eq(const uint32_t* __restrict__ p, uint32_t
 #define MYERS_SHIFT_MODE 0
 #endif
 
-// Multipliers 1 and 2 read from the kernel parameters: ptxas cannot fold them
-// into shifts or adds, so multiply-adds by them stay on the FMA pipe.
+// Multipliers read from the kernel parameters. ptxas cannot fold them into
+// shifts or adds, so multiply-adds by them execute on the FMA pipe, which the
+// Myers recurrence leaves idle (it saturates the integer ALU pipe). The
+// per-column bookkeeping -- score update, text code extraction, shared
+// memory addressing, lane masks -- runs there.
 struct Mul {
-  uint32_t one, two;
+  uint32_t one, two;   // 1, 2
+  uint32_t k16, mk16;  // 1 << 16, -(1 << 16)
+  uint32_t p28;        // 1 << 28: umulhi(x, p28) = x >> 4
+  uint32_t kb33, kb17; // bytes between bases of a group for 33 / 17 columns
 };
+
+__device__ __forceinline__ Mul make_mul(const DevInputs& in) {
+  return Mul{in.one, in.two, in.k16, in.mk16, in.p28, in.kb33, in.kb17};
+}
+
+// Score key update for one column on the FMA pipe: the top row's Ph / Mh bit
+// 31 add +1 / -1 to the score held in bits 16..31 of sc.
+__device__ __forceinline__ uint32_t score_step(uint32_t sc, uint32_t tp, uint32_t tm, Mul k) {
+  const uint32_t hp = __umulhi(tp, k.two);
+  const uint32_t hm = __umulhi(tm, k.two);
+  sc = hp * k.k16 + sc;
+  return hm * k.mk16 + sc;
+}
+
+// Bytes between the bases of a PEQ group for shape (W, MULTI).
+template <int W, bool MULTI>
+__device__ __forceinline__ uint32_t base_bytes(Mul k) {
+  static_assert(Layout<W, MULTI>::NCOL == 33 || Layout<W, MULTI>::NCOL == 17, "column count");
+  return Layout<W, MULTI>::NCOL == 33 ? k.kb33 : k.kb17;
+}
 
 // s = a + b over W words with the carry rippling through the CC flag.
 template <int W>
@@ -185,7 +211,7 @@ template <int W, bool HIN>
 __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (&Pv)[W], uint32_t (&Mv)[W],
                                              uint32_t inP, uint32_t inM, uint32_t& topP, uint32_t& topM, Mul k) {
   uint32_t e0 = eq[0];
-  if (HIN) e0 |= inM >> 31;
+  if (HIN) e0 |= __umulhi(inM, k.two);  // inM >> 31
   uint32_t t[W], s[W];
   t[0] = e0 & Pv[0];
 #pragma unroll
@@ -212,21 +238,52 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
 }
 
 // Eight columns of one text word, single-lane shapes. TAIL masks columns >= n.
+// Eight columns of one text word (codes 0..4 in its nibbles), single-lane
+// shapes. TAIL masks columns >= n.
 template <int W, bool TAIL>
 __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                               uint32_t (&Mv)[W], uint32_t& sc, uint32_t& kmin,
                                               uint32_t colbase, uint32_t n, Mul k) {
+  const uint32_t kb = base_bytes<W, false>(k);
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const uint32_t off = ((t >> (4 * u)) & 7u) * (uint32_t)(Layout<W, false>::BASE * 4);
+    const uint32_t code = t & 7u;
+    if (u < 7) t = __umulhi(t, k.p28);  // next nibble
     uint32_t eq[W];
-    load_eq<W, false>(reinterpret_cast<const uint32_t*>(slot + off), eq);
+    load_eq<W, false>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
     uint32_t tp, tm;
     myers_column<W, false>(eq, Pv, Mv, 0u, 0u, tp, tm, k);
-    sc += (tp >> 31) << 16;
-    sc -= (tm >> 31) << 16;
+    sc = score_step(sc, tp, tm, k);
     const uint32_t key = sc + colbase + (uint32_t)u;
     if (!TAIL || colbase + (uint32_t)u < n) kmin = min(kmin, key);
+  }
+}
+
+// Eight systolic steps of a multi-lane shape. CHECKED: some lanes may be
+// outside their candidate's columns (pipeline fill and drain, shorter
+// candidates); otherwise every lane with work is inside (steady state), and
+// lanes without work compute values nobody reads.
+template <int W, bool CHECKED>
+__device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
+                                             uint32_t (&Mv)[W], uint32_t& outP, uint32_t& outM, uint32_t& sc,
+                                             uint32_t& kmin, uint32_t jbase, uint32_t n, bool work,
+                                             uint32_t segmul, Mul k) {
+  const uint32_t kb = base_bytes<W, true>(k);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const uint32_t code = t & 7u;
+    if (u < 7) t = __umulhi(t, k.p28);
+    uint32_t eq[W];
+    load_eq<W, true>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
+    // the bottom lane of a segment takes no delta (segmul 0)
+    const uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1) * segmul;
+    const uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1) * segmul;
+    const uint32_t j = jbase + (uint32_t)u;  // wraps when negative
+    if (!CHECKED || (work && j < n)) {
+      myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM, k);
+      sc = score_step(sc, outP, outM, k);
+      kmin = min(kmin, sc + j);
+    }
   }
 }
 
@@ -321,7 +378,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
   const long long q0 = (long long)(in.exact ? c.pos : (c.pos & ~7ull)) - l;
   const long long b0 = q0 >> 3;
   const uint32_t sh = 4u * (uint32_t)(q0 & 7);
-  const Mul k{in.one, in.two};
+  const Mul k = make_mul(in);
 
   for (int r = 0; r < rounds; ++r) {
     const int slot = run - r * (Lay::SLOTS / Lr);
@@ -363,34 +420,22 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
     } else {
       uint32_t steps = work ? c.n + (uint32_t)L - 1u : 0u;
       steps = __reduce_max_sync(FULL_MASK, steps);
+      // steps [L-1, n_min) have every lane with work inside its columns
+      const uint32_t n_min = __reduce_min_sync(FULL_MASK, work ? c.n : 0xFFFFFFFFu);
       const uint32_t nblk = (steps + 7u) >> 3;
       uint32_t lo = ref_load(in.ref, b0, in.ref_words);
       uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
       uint32_t outP = 0u, outM = 0u;
-      const bool seg_start = (l == 0);
+      const uint32_t segmul = (uint32_t)min(l, 1);
       for (uint32_t i = 0; i < nblk; ++i) {
         const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
         lo = hi;
         hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const uint32_t off = ((t >> (4 * u)) & 7u) * (uint32_t)(Lay::BASE * 4);
-          uint32_t eq[W];
-          load_eq<W, true>(reinterpret_cast<const uint32_t*>(slotp + off), eq);
-          uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1);
-          uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1);
-          if (seg_start) {
-            inP = 0u;
-            inM = 0u;
-          }
-          const uint32_t j = 8u * i + (uint32_t)u - (uint32_t)l;  // wraps when negative
-          if (work && j < c.n) {
-            myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM, k);
-            sc += (outP >> 31) << 16;
-            sc -= (outM >> 31) << 16;
-            kmin = min(kmin, sc + j);
-          }
-        }
+        const uint32_t jbase = 8u * i - (uint32_t)l;
+        if (8u * i + 1u >= (uint32_t)L && 8u * i + 8u <= n_min)
+          block8_multi<W, false>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
+        else
+          block8_multi<W, true>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
       }
       if (work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
     }
@@ -530,7 +575,10 @@ __device__ __forceinline__ void dispatch(int v, const DevInputs& in, const uint3
 // Each warp pulls the next tile index from the device queue; tiles are
 // ordered by shape, most expensive shape first, so the long candidates start
 // early and the short ones fill the tail.
-__global__ void __launch_bounds__(128) k_batched(DevInputs in, const uint32_t* __restrict__ ids,
+#ifndef MYERS_BATCHED_MIN_BLOCKS
+#define MYERS_BATCHED_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(128, MYERS_BATCHED_MIN_BLOCKS) k_batched(DevInputs in, const uint32_t* __restrict__ ids,
                                                  const __grid_constant__ PlanTable plan, BucketState* st) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint32_t s_tile_start[kMaxCfg + 1];
