@@ -444,12 +444,24 @@ def run_serving(args):
     # serving gap into shape cost and serving-loop cost
     same_cps = None
     if args.lane_words > 0:
-        widths = sorted(W for v, W, multi in mg.variants() if multi and W <= 16)
-        Wl = min([W for W in widths if W >= args.lane_words] or [widths[-1]])
-        v_l = [v for v, W, multi in mg.variants() if multi and W == Wl][0]
+        # the server's latency policy: the cheapest multi-lane shape with lanes
+        # of at most lane_words words (lanes x (10W + 16) per column step)
+        multi = [(v, W) for v, W, m in mg.variants() if m and W <= 16]
+
+        def latency_shape(wd):
+            best = None
+            for v, W in multi:
+                L = -(-wd // W)
+                if (W > args.lane_words and W != multi[0][1]) or not 2 <= L <= 32:
+                    continue
+                cost = (32.0 / (32 // L)) * (10 * W + 16)
+                if best is None or cost < best[0]:
+                    best = (cost, v, L)
+            return best[1], best[2]
+
         words = range(args.lane_words + 1, 33)
         for wd in words:
-            mg.set_shape_override(mg.PATH_BATCHED, wd, v_l, -(-wd // Wl))
+            mg.set_shape_override(mg.PATH_BATCHED, wd, *latency_shape(wd))
         for _ in range(2):
             step()
         a.record(st)

@@ -108,8 +108,8 @@ def main():
         sampled = sorted(measured[pname])
         for w in range(1, 1025):
             if w in measured[pname]:
-                v, L, _ = measured[pname][w]["shape"]
-                table[pname][w] = [v, L]
+                v, L, W = measured[pname][w]["shape"]
+                table[pname][w] = [W, L]
                 continue
             above = [x for x in sampled if x >= w]
             ref_w = above[0] if above else sampled[-1]
@@ -123,12 +123,13 @@ def main():
                     continue
                 L2 = math.ceil(w / W2)
                 if 2 <= L2 <= 32:
-                    table[pname][w] = [widths[W2], L2]
+                    table[pname][w] = [W2, L2]
                     break
     props = torch.cuda.get_device_properties(0)
     out = {"device": props.name, "sms": props.multi_processor_count, "distance": DIST,
            "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
            "method": "per bucket: every compiled shape timed on reads of 32*w bases, best of 3 after a warm-up",
+           "format": "plain/batched: words -> [W words per lane, L lanes per candidate]",
            "plain": {str(k): v for k, v in table["plain"].items()},
            "batched": {str(k): v for k, v in table["batched"].items()},
            "measured": {p: {str(k): v for k, v in measured[p].items()} for p in measured}}

@@ -184,8 +184,9 @@ static Override g_tuned[2][kMaxWords + 1];  // from the autotuner's cache file
 
 // Load the autotuner's cache: `autotune_b200.json` next to this library (or
 // the file named by MYERS_AUTOTUNE; MYERS_AUTOTUNE=0 disables it). Format:
-// {"plain": {"<words>": [variant, L], ...}, "batched": {...}, ...}; entries
-// that name a shape the path cannot run are ignored.
+// {"plain": {"<words>": [W, L], ...}, "batched": {...}, ...} with W words per
+// lane and L lanes per candidate; entries naming a shape that is not compiled
+// or that the path cannot run are ignored.
 static void load_tuned_once() {
   static std::once_flag once;
   std::call_once(once, [] {
@@ -220,11 +221,17 @@ static void load_tuned_once() {
       const char* e = text.c_str() + end;
       while (p < e) {
         unsigned w = 0;
-        int v = -1, L = 0, used = 0;
-        if (sscanf(p, " \"%u\" : [ %d , %d ]%n", &w, &v, &L, &used) == 3 && used > 0) {
-          if (w >= 1 && w <= kMaxWords && v >= 0 && v < kNumVariants && L >= 1 && L <= 32 &&
-              (uint32_t)(variant_W(v) * (variant_multi(v) ? L : 1)) >= w && (path_id == 0 || batched_supports(v)))
-            g_tuned[path_id][w] = Override{true, (uint8_t)v, (uint8_t)(variant_multi(v) ? L : 1)};
+        int W = 0, L = 0, used = 0;
+        if (sscanf(p, " \"%u\" : [ %d , %d ]%n", &w, &W, &L, &used) == 3 && used > 0) {
+          // [W, L]: L == 1 is one candidate per lane with W words, L >= 2 a
+          // candidate over L lanes of W words
+          int v = -1;
+          if (L == 1 && W >= 1 && W <= kNumSingle) v = W - 1;
+          for (int mi = 0; L >= 2 && mi < kNumMulti; ++mi)
+            if (kMultiW[mi] == W) v = kNumSingle + mi;
+          if (v >= 0 && w >= 1 && w <= kMaxWords && L <= 32 && (uint32_t)(W * L) >= w &&
+              (path_id == 0 || batched_supports(v)))
+            g_tuned[path_id][w] = Override{true, (uint8_t)v, (uint8_t)L};
           p += used;
         } else {
           ++p;
@@ -246,12 +253,22 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
     if (o.set) return Shape{o.variant, o.L, (uint8_t)variant_W(o.variant), 0};
   }
   if (lane_words > 0 && w > lane_words) {
+    // the cheapest multi-lane shape whose lanes hold at most lane_words words
+    // (the smallest width if none does)
+    double best = 1e300;
+    Shape bs{0, 0, 0, 0};
     for (int mi = 0; mi < kNumMulti; ++mi) {
       const uint32_t W = (uint32_t)kMultiW[mi];
-      if (W < lane_words || (batched && W > (uint32_t)kBatchedMaxMultiW)) continue;
+      if ((W > lane_words && mi > 0) || (batched && W > (uint32_t)kBatchedMaxMultiW)) continue;
       const uint32_t L = (w + W - 1) / W;
-      if (L >= 2 && L <= 32) return Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};
+      if (L < 2 || L > 32) continue;
+      const double c = shape_cost(kNumSingle + mi, (int)L);
+      if (c < best) {
+        best = c;
+        bs = Shape{(uint8_t)(kNumSingle + mi), (uint8_t)L, (uint8_t)W, 0};
+      }
     }
+    if (bs.L) return bs;
   }
   {
     std::lock_guard<std::mutex> lk(g_override_mu);

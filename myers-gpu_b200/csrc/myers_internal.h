@@ -32,7 +32,7 @@ struct Cand {
 // candidate over L lanes of W words and hand the horizontal delta from lane
 // to lane once per column.
 constexpr int kNumSingle = 32;
-constexpr int kMultiW[] = {4, 6, 8, 10, 12, 16, 32};
+constexpr int kMultiW[] = {4, 5, 6, 7, 8, 10, 12, 16, 32};
 constexpr int kNumMulti = sizeof(kMultiW) / sizeof(kMultiW[0]);
 constexpr int kNumVariants = kNumSingle + kNumMulti;
 // The persistent kernel carries every single-lane shape and multi-lane

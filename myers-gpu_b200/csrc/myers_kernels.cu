@@ -240,15 +240,15 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
 // Eight columns of one text word, single-lane shapes. TAIL masks columns >= n.
 // Eight columns of one text word (codes 0..4 in its nibbles), single-lane
 // shapes. TAIL masks columns >= n.
-template <int W, bool TAIL>
+template <int W, bool TAIL, int UNR>
 __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                               uint32_t (&Mv)[W], uint32_t& sc, uint32_t& kmin,
                                               uint32_t colbase, uint32_t n, Mul k) {
   const uint32_t kb = base_bytes<W, false>(k);
-#pragma unroll
+#pragma unroll UNR
   for (int u = 0; u < 8; ++u) {
     const uint32_t code = t & 7u;
-    if (u < 7) t = __umulhi(t, k.p28);  // next nibble
+    t = __umulhi(t, k.p28);  // next nibble
     uint32_t eq[W];
     load_eq<W, false>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
     uint32_t tp, tm;
@@ -263,16 +263,16 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
 // outside their candidate's columns (pipeline fill and drain, shorter
 // candidates); otherwise every lane with work is inside (steady state), and
 // lanes without work compute values nobody reads.
-template <int W, bool CHECKED>
+template <int W, bool CHECKED, int UNR>
 __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                              uint32_t (&Mv)[W], uint32_t& outP, uint32_t& outM, uint32_t& sc,
                                              uint32_t& kmin, uint32_t jbase, uint32_t n, bool work,
                                              uint32_t segmul, Mul k) {
   const uint32_t kb = base_bytes<W, true>(k);
-#pragma unroll
+#pragma unroll UNR
   for (int u = 0; u < 8; ++u) {
     const uint32_t code = t & 7u;
-    if (u < 7) t = __umulhi(t, k.p28);
+    t = __umulhi(t, k.p28);
     uint32_t eq[W];
     load_eq<W, true>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
     // the bottom lane of a segment takes no delta (segmul 0)
@@ -349,7 +349,10 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
   return c;
 }
 
-template <int W, bool MULTI>
+// UNR: how far the 8 columns of a text word are unrolled -- fully for the
+// one-shape plain kernels; partly in the persistent kernel, whose code holds
+// every shape and would otherwise overflow the instruction cache.
+template <int W, bool MULTI, int UNR = 8>
 __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
                                              uint32_t cnt, int L, uint32_t* __restrict__ wsmem, int lane) {
   using Lay = Layout<W, MULTI>;
@@ -409,11 +412,11 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
           const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
           lo = hi;
           hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
-          block8_single<W, false>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
+          block8_single<W, false, UNR>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
         }
         if (c.n & 7u) {
           const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
-          block8_single<W, true>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
+          block8_single<W, true, UNR>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
         }
         in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
       }
@@ -433,9 +436,9 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
         hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
         const uint32_t jbase = 8u * i - (uint32_t)l;
         if (8u * i + 1u >= (uint32_t)L && 8u * i + 8u <= n_min)
-          block8_multi<W, false>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
+          block8_multi<W, false, UNR>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
         else
-          block8_multi<W, true>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
+          block8_multi<W, true, UNR>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
       }
       if (work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
     }
@@ -555,14 +558,18 @@ constexpr uint32_t cmax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 constexpr uint32_t kBatchedWarpWords =
     cmax(cmax(warp_words<32, false>(), warp_words<16, false>()), warp_words<kBatchedMaxMultiW, true>());
 
+#ifndef MYERS_BATCHED_UNROLL
+#define MYERS_BATCHED_UNROLL 2
+#endif
+
 template <int V>
 __device__ __forceinline__ void dispatch_one(const DevInputs& in, const uint32_t* ids, uint32_t f, uint32_t cnt,
                                              int L, uint32_t* wsmem, int lane) {
   if constexpr (V < kNumSingle) {
-    process_tile<V + 1, false>(in, ids, f, cnt, L, wsmem, lane);
+    process_tile<V + 1, false, MYERS_BATCHED_UNROLL>(in, ids, f, cnt, L, wsmem, lane);
   } else {
     if constexpr (kMultiW[V - kNumSingle] <= kBatchedMaxMultiW)
-      process_tile<kMultiW[V - kNumSingle], true>(in, ids, f, cnt, L, wsmem, lane);
+      process_tile<kMultiW[V - kNumSingle], true, MYERS_BATCHED_UNROLL>(in, ids, f, cnt, L, wsmem, lane);
   }
 }
 

@@ -371,6 +371,71 @@ extern "C" int myersServerCreate(myersServer_t** out, const myersReference_t* re
   return MYERS_SUCCESS;
 }
 
+namespace {
+struct SubmitItem {
+  const qryEntry_t* peq;
+  uint32_t m;
+  const uint64_t* pos;
+  uint32_t ncand;
+};
+}  // namespace
+
+// Queue n requests under one lock round (the replay driver uses it when
+// several requests are due at once). status[i] / ticket[i] per request.
+static void submit_many(myersServer* srv, const SubmitItem* it, uint32_t n, int* status, uint64_t* ticket) {
+  Request* reqs[256];
+  uint32_t ok = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    status[i] = MYERS_SUCCESS;
+    if (it[i].m > srv->cfg.maxQuerySize) status[i] = MYERS_E_QUERY_TOO_LONG;
+    else if (it[i].ncand > srv->cap_cands || entries_of(it[i].m) > srv->cap_entries) status[i] = MYERS_E_CAPACITY;
+  }
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    for (uint32_t i = 0; i < n; ++i) {
+      reqs[i] = nullptr;
+      if (status[i] != MYERS_SUCCESS) continue;
+      if (srv->stop) status[i] = MYERS_E_INVALID_ARGUMENT;
+      else if (srv->fatal != MYERS_SUCCESS) status[i] = srv->fatal;
+      else if (srv->pending.size() + ok >= srv->cfg.maxQueued) {
+        srv->stats.refused++;
+        status[i] = MYERS_E_BUSY;
+      } else {
+        ++ok;
+        if (!srv->free_reqs.empty()) {
+          reqs[i] = srv->free_reqs.back();
+          srv->free_reqs.pop_back();
+        }
+      }
+    }
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    if (status[i] != MYERS_SUCCESS) continue;
+    Request* r = reqs[i] ? reqs[i] : new Request();
+    r->m = it[i].m;
+    r->state = kPending;
+    r->status = MYERS_SUCCESS;
+    r->peq.assign(it[i].peq, it[i].peq + entries_of(it[i].m));
+    r->pos.assign(it[i].pos, it[i].pos + it[i].ncand);
+    reqs[i] = r;
+  }
+  bool wake = false;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    for (uint32_t i = 0; i < n; ++i) {
+      if (status[i] != MYERS_SUCCESS) continue;
+      Request* r = reqs[i];
+      r->ticket = srv->next_ticket++;
+      srv->live[r->ticket] = r;
+      srv->pending.push_back(r);
+      srv->stats.submitted++;
+      ticket[i] = r->ticket;
+    }
+    wake = srv->want_requests && ok > 0;
+  }
+  if (wake) srv->cv_dispatch.notify_one();
+}
+
 extern "C" int myersServerSubmit(myersServer_t* srv, const qryEntry_t* peq, uint32_t querySize,
                                  const uint64_t* positions, uint32_t numCandidates, uint64_t* ticket) {
   if (srv == nullptr || ticket == nullptr || (querySize > 0 && peq == nullptr) ||
@@ -472,14 +537,28 @@ extern "C" int myersServerReplay(myersServer_t* srv, const qryEntry_t* peq, cons
     return MYERS_E_INVALID_ARGUMENT;
   std::vector<uint64_t> tickets(numRequests, 0);
   std::vector<int> ok(numRequests, 0);
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->live.reserve(srv->live.size() + numRequests);
+  }
   const uint64_t t0 = now_ns() + 1000000;  // start 1 ms from now
-  for (uint32_t i = 0; i < numRequests; ++i) {
+  SubmitItem items[256];
+  int st[256];
+  for (uint32_t i = 0; i < numRequests;) {
     const uint64_t due = t0 + arrivalNs[i];
-    while (now_ns() < due) {
+    uint64_t now = now_ns();
+    while (now < due) now = now_ns();
+    // every request already due goes in one round
+    uint32_t n = 0;
+    while (i + n < numRequests && n < 256 && t0 + arrivalNs[i + n] <= now) {
+      const uint32_t q = i + n;
+      items[n] = SubmitItem{peq + qinfo[q].posEntry, qinfo[q].size, positions + candOffset[q],
+                            candOffset[q + 1] - candOffset[q]};
+      ++n;
     }
-    const int st = myersServerSubmit(srv, peq + qinfo[i].posEntry, qinfo[i].size, positions + candOffset[i],
-                                     candOffset[i + 1] - candOffset[i], &tickets[i]);
-    ok[i] = st == MYERS_SUCCESS;
+    submit_many(srv, items, n, st, tickets.data() + i);
+    for (uint32_t k = 0; k < n; ++k) ok[i + k] = st[k] == MYERS_SUCCESS;
+    i += n;
   }
   uint64_t last = t0;
   int status = MYERS_SUCCESS;
