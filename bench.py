@@ -47,7 +47,7 @@ WORKLOAD_NAMES = {
     2: "plain-1000b: 3.1 Gbase ref, 1M reads x 1000 b, 11 cand/read (11M candidates)",
     3: "batched-mixed: 3.1 Gbase ref, 2M reads of 100..1000 b, 1+Poisson(10) cand/read",
     4: "batched-long: 3.1 Gbase ref, 100K reads of 1000..10000 b, 1+Poisson(4) cand/read",
-    5: "serving-mix: 3.1 Gbase ref, reads of 100..1000 b, 1..64 cand/read",
+    5: "serving-mix: 3.1 Gbase ref, 300K requests of one read (100..1000 b) and 1..64 candidates",
 }
 
 
@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--lane-words", type=int, default=8, help="serving: words per lane of the latency shapes")
+    ap.add_argument("--lane-words", type=int, default=12, help="serving: words per lane of the latency shapes")
     ap.add_argument("--slots", type=int, default=4, help="serving: batches in flight")
     ap.add_argument("--no-graphs", action="store_true", help="serving: launch batches without CUDA graphs")
     return ap.parse_args()
@@ -410,7 +410,8 @@ def run_serving(args):
     if rank != 0:
         return
     torch.cuda.set_device(0)
-    s, ref_words, ref_size, w = make_inputs(mg, 5, args.scale, 0)
+    # a pool of 300K requests (~9.8M candidates): ~0.1 s of load at the top rates
+    s, ref_words, ref_size, w = make_inputs(mg, 5, 3.0 * args.scale, 0)
     off = np.concatenate([[0], np.cumsum(w["ncands"])]).astype(np.uint32)
     n_req, n_cands = len(w["qinfo"]), len(w["cands"])
     mean_c = n_cands / n_req
@@ -475,7 +476,9 @@ def run_serving(args):
     ctx.close()
     del d_peq, d_qi, d_c, d_res
 
-    rates = [1e4, 1e5, 1e6, 2e6, 5e6, 1e7, 2e7, 3e7, 4e7, 5e7, 5.5e7, 6e7, 6.5e7, 7e7, 7.5e7, 8e7]
+    rates = [1e4, 1e5, 1e6, 2e6, 5e6, 1e7, 2e7, 3e7, 4e7, 5e7, 6e7, 7e7, 7.5e7, 8e7, 8.2e7, 8.4e7, 8.6e7, 8.8e7,
+             9e7, 9.2e7, 9.5e7, 1e8,
+             1.1e8]
     rng = np.random.default_rng(5)
     sweep, same = [], True
     clocks = ClockSampler(0)
