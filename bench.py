@@ -86,6 +86,15 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.skip = 0
+        self.pokes = []
+        self.nvml = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = (pynvml, pynvml.nvmlDeviceGetHandleByIndex(gpu_index))
+        except Exception:  # no NVML: the nvidia-smi rows alone
+            self.nvml = None
 
     def start(self):
         try:
@@ -94,18 +103,41 @@ class ClockSampler:
                                          stdout=self.out, stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+            return
+        # wait for the first row, so that the sampler runs when the timed region starts;
+        # rows written before the region are dropped
+        t0 = time.time()
+        while time.time() - t0 < 5 and os.path.getsize(self.out.name) == 0:
+            time.sleep(0.01)
+        self.out.flush()
+        self.skip = len(open(self.out.name).read().strip().splitlines())
+
+    def poke(self):
+        """One NVML reading, taken while queued steps run (covers timed regions
+        shorter than the sampler's 200 ms period)."""
+        if self.nvml is None:
+            return
+        nv, h = self.nvml
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        except Exception:
+            return
+        masks = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+        self.pokes.append((float(sm), float(smax), {n for n, m in masks.items() if bits & m}))
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.out.flush()
-        self.out.seek(0)
-        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        rows = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.flush()
+            self.out.seek(0)
+            rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()][self.skip:]
         os.unlink(self.out.name)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -118,6 +150,10 @@ class ClockSampler:
                         reasons.add(name)
             except (ValueError, IndexError):
                 continue
+        for c, cmax, rs in self.pokes:
+            sm.append(c)
+            smax = cmax
+            reasons |= rs
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
@@ -279,17 +315,22 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
+    # L2 is flushed (a 256 MiB write, outside the events) before every timed step
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     clocks.start()
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    evs[0].record(stream)
-    for i in range(args.steps):
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in evs:
+        flush.zero_()
+        a.record(stream)
         step()
-        evs[i + 1].record(stream)
+        b.record(stream)
+    clocks.poke()
     torch.cuda.synchronize()
     clk = clocks.stop()
+    del flush
     if dist is not None:
         dist.barrier()
-    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    step_ms = [a.elapsed_time(b) for a, b in evs]
     elapsed = sum(step_ms) / 1e3
     if dist is not None:
         elapsed, all_cands, all_cells = reduce_over_ranks(dist, elapsed, n_cands, cells.sum(), "cuda")
@@ -340,8 +381,7 @@ def run_ours(args):
             "gcups": gcups,
             "config": {"workload": WORKLOAD_NAMES[k], "candidates_per_gpu": n_cands, "distance": DIST,
                        "window": "aligned", "path": "batched" if path == mg.PATH_BATCHED else "plain",
-                       "l2": "inputs larger than L2 (3.1 Gbase reference = 1.55 GB resident)" if k != 1
-                       else "16 Mbase reference fits L2; candidates/PEQ stream from HBM",
+                       "l2": "L2 flushed before every timed step (256 MiB write, untimed)",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -382,16 +422,22 @@ def run_e2e(mg, args, ref_words, ref_size, w, path):
         for _ in range(max(1, args.warmup)):
             bufs.send(0, DIST, len(w["peq"]), len(w["qinfo"]), n_cands)
             mg.check(bufs.receive(0), "receive")
-        t = time.perf_counter()
+        import torch
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        el = 0.0
         for _ in range(args.steps):
+            flush.zero_()  # L2 flushed before every step, outside the timed call
+            torch.cuda.synchronize()
+            t = time.perf_counter()
             bufs.send(0, DIST, len(w["peq"]), len(w["qinfo"]), n_cands)
             mg.check(bufs.receive(0), "receive")
-        el = time.perf_counter() - t
+            el += time.perf_counter() - t
+        del flush
         h2d = len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * 16
         return {"value": n_cands * args.steps / el, "unit": "candidates/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(n_cands * 8),
                 "api": "initMyers buffers: fill pinned host buffers (untimed), then sendMyersBuffer + "
-                       "receiveMyersBuffer per step (H2D, kernels, D2H timed)"}
+                       "receiveMyersBuffer per step (H2D, kernels, D2H timed on the host clock; L2 flushed between steps)"}
     finally:
         bufs.close()
         mg.lib.myersSetMemoryBudget(0)

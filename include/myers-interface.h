@@ -143,7 +143,9 @@ enum { MYERS_WINDOW_ALIGNED = 0, MYERS_WINDOW_EXACT = 1 };
  *  PLAIN: one launch per length bucket present (the fixed-length kernel;
  *    a single launch when all queries share one bucket).
  *  BATCHED: one persistent launch pulling length-bucketed work tiles from a
- *    device queue, replayed from a CUDA graph. */
+ *    device queue.
+ * A buffer's send (copies in, kernels, copies out) is captured and replayed
+ * as one CUDA graph, updated in place from send to send (myersSetGraphs). */
 enum { MYERS_PATH_PLAIN = 0, MYERS_PATH_BATCHED = 1 };
 
 /* Status-returning versions of the main calls: same behaviour, but errors
@@ -158,6 +160,9 @@ int myersEnd(void ***myersBuffer);
 /* Per-buffer options; take effect at the next send. */
 int myersSetWindowMode(void *myersBuffer, int mode);
 int myersSetKernelPath(void *myersBuffer, int path);
+/* Non-zero (default): replay each send as a CUDA graph; 0: plain stream
+ * launches. The environment variable MYERS_GRAPHS=0 sets the default to 0. */
+int myersSetGraphs(void *myersBuffer, int enable);
 
 /* Device memory budget (bytes) for all buffers created by the next
  * initMyers/myersInit, replacing the reference's "95% of free memory"

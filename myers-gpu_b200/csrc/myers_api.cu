@@ -656,6 +656,8 @@ struct Buffer {
   resEntry_t* d_results;
   int window_mode;
   int path;
+  int use_graphs;
+  cudaGraphExec_t exec;  // the last send, updated in place by the next
   int last_status;
   bool pending;
   std::vector<uint8_t> present;  // word counts of the last send
@@ -685,6 +687,7 @@ static void buffer_free(Buffer* b) {
   cudaFree(b->d_qinfo);
   cudaFree(b->d_cands);
   cudaFree(b->d_results);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->ctx) myersContextDestroy(b->ctx);
   if (b->stream) cudaStreamDestroy(b->stream);
   if (b->shared && --b->shared->refs == 0) {
@@ -756,6 +759,8 @@ extern "C" int myersInit(void*** myersBuffer, uint32_t numBuffers, const char* r
     b->path = MYERS_PATH_PLAIN;
     const char* p = getenv("MYERS_PATH");
     if (p && strcmp(p, "batched") == 0) b->path = MYERS_PATH_BATCHED;
+    const char* g = getenv("MYERS_GRAPHS");
+    b->use_graphs = !(g && strcmp(g, "0") == 0);
     b->present.assign(kMaxWords + 1, 0);
     bufs[i] = b;
     st = buffer_alloc(b);
@@ -795,25 +800,38 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
   int st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
   if (st != MYERS_SUCCESS) return b->last_status = st;
   cudaStream_t s = b->stream;
-  CU(cudaMemsetAsync(b->ctx->d_flags, 0, 4, s));
-  CU(cudaMemcpyAsync(b->d_peq, b->h_peq, (size_t)numPEQEntries * sizeof(qryEntry_t), cudaMemcpyHostToDevice, s));
-  CU(cudaMemcpyAsync(b->d_qinfo, b->h_qinfo, (size_t)numQueries * sizeof(qryInfo_t), cudaMemcpyHostToDevice, s));
-  CU(cudaMemcpyAsync(b->d_cands, b->h_cands, (size_t)numCandidates * sizeof(candInfo_t), cudaMemcpyHostToDevice, s));
-  DevInputs in;
-  memset(&in, 0, sizeof(in));
-  in.peq = reinterpret_cast<const uint32_t*>(b->d_peq);
-  in.qinfo = reinterpret_cast<const uint2*>(b->d_qinfo);
-  in.cands = reinterpret_cast<const Cand*>(b->d_cands);
-  in.results = reinterpret_cast<uint2*>(b->d_results);
-  in.num_cands = numCandidates;
-  in.num_queries = numQueries;
-  in.num_entries = numPEQEntries;
-  in.distance = distance;
-  in.exact = b->window_mode == MYERS_WINDOW_EXACT;
-  st = verify_enqueue(b->ctx, b->shared->ref, in, plan, b->path, s);
+  auto enqueue = [&]() -> int {
+    CU(cudaMemsetAsync(b->ctx->d_flags, 0, 4, s));
+    if (numCandidates == 0) {  // nothing to verify: only the flags travel back
+      CU(cudaMemcpyAsync(b->h_flags, b->ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
+      return MYERS_SUCCESS;
+    }
+    if (numPEQEntries)
+      CU(cudaMemcpyAsync(b->d_peq, b->h_peq, (size_t)numPEQEntries * sizeof(qryEntry_t), cudaMemcpyHostToDevice, s));
+    if (numQueries)
+      CU(cudaMemcpyAsync(b->d_qinfo, b->h_qinfo, (size_t)numQueries * sizeof(qryInfo_t), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(b->d_cands, b->h_cands, (size_t)numCandidates * sizeof(candInfo_t), cudaMemcpyHostToDevice,
+                       s));
+    DevInputs in;
+    memset(&in, 0, sizeof(in));
+    in.peq = reinterpret_cast<const uint32_t*>(b->d_peq);
+    in.qinfo = reinterpret_cast<const uint2*>(b->d_qinfo);
+    in.cands = reinterpret_cast<const Cand*>(b->d_cands);
+    in.results = reinterpret_cast<uint2*>(b->d_results);
+    in.num_cands = numCandidates;
+    in.num_queries = numQueries;
+    in.num_entries = numPEQEntries;
+    in.distance = distance;
+    in.exact = b->window_mode == MYERS_WINDOW_EXACT;
+    const int est = verify_enqueue(b->ctx, b->shared->ref, in, plan, b->path, s);
+    if (est != MYERS_SUCCESS) return est;
+    CU(cudaMemcpyAsync(b->h_results, b->d_results, (size_t)numCandidates * sizeof(resEntry_t),
+                       cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(b->h_flags, b->ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
+    return MYERS_SUCCESS;
+  };
+  st = b->use_graphs ? launch_as_graph(s, &b->exec, enqueue) : enqueue();
   if (st != MYERS_SUCCESS) return b->last_status = st;
-  CU(cudaMemcpyAsync(b->h_results, b->d_results, (size_t)numCandidates * sizeof(resEntry_t), cudaMemcpyDeviceToHost, s));
-  CU(cudaMemcpyAsync(b->h_flags, b->ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
   b->pending = true;
   return MYERS_SUCCESS;
 }
@@ -860,6 +878,13 @@ extern "C" int myersSetKernelPath(void* mb, int path) {
   Buffer* b = static_cast<Buffer*>(mb);
   if (b == nullptr || (path != MYERS_PATH_PLAIN && path != MYERS_PATH_BATCHED)) return MYERS_E_INVALID_ARGUMENT;
   b->path = path;
+  return MYERS_SUCCESS;
+}
+
+extern "C" int myersSetGraphs(void* mb, int enable) {
+  Buffer* b = static_cast<Buffer*>(mb);
+  if (b == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  b->use_graphs = enable != 0;
   return MYERS_SUCCESS;
 }
 

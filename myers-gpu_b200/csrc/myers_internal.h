@@ -174,4 +174,39 @@ namespace myers {
 // Enqueue the kernels of one batch on stream s (inputs already on the device).
 int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in, const PlanTable& plan, int path,
                    cudaStream_t s);
+
+// Capture what enqueue() puts on stream s and launch it as the graph *exec.
+// Consecutive batches differ only in copy sizes and kernel arguments, so the
+// executable graph is updated in place; when the topology changed (another
+// set of length buckets on the plain path) it is instantiated anew. The
+// capture is always ended, also when enqueue() fails.
+template <class F>
+int launch_as_graph(cudaStream_t s, cudaGraphExec_t* exec, F&& enqueue) {
+  cudaError_t ce = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamBeginCapture");
+  const int st = enqueue();
+  cudaGraph_t g = nullptr;
+  ce = cudaStreamEndCapture(s, &g);
+  if (st != 0 || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return st != 0 ? st : cuda_fail(ce, "cudaStreamEndCapture");
+  }
+  if (*exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(*exec, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(*exec);
+      *exec = nullptr;
+    }
+  }
+  if (*exec == nullptr && (ce = cudaGraphInstantiate(exec, g, 0)) != cudaSuccess) {
+    *exec = nullptr;
+    cudaGraphDestroy(g);
+    return cuda_fail(ce, "cudaGraphInstantiate");
+  }
+  cudaGraphDestroy(g);
+  ce = cudaGraphLaunch(*exec, s);
+  return ce == cudaSuccess ? 0 : cuda_fail(ce, "cudaGraphLaunch");
+}
 }  // namespace myers

@@ -153,34 +153,11 @@ static int dispatch_slot(myersServer* srv, Slot& s) {
   int st = build_plan(plan, present, srv->cfg.path == MYERS_PATH_BATCHED, srv->cfg.laneWords);
   if (st != MYERS_SUCCESS) return st;
   // With graphs, the batch's copies and kernels are captured and replayed as
-  // one graph: the captured graph only differs from the slot's previous one
-  // in sizes and kernel arguments, so the executable graph is updated in
-  // place and relaunched.
-  const bool graph = srv->cfg.useGraphs != 0;
-  if (graph && cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) return MYERS_E_CUDA;
-  st = enqueue_batch(srv, s, plan, ne, nq, nc);
-  if (graph) {
-    cudaGraph_t g = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(s.stream, &g);
-    if (st != MYERS_SUCCESS || ce != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      return st != MYERS_SUCCESS ? st : cuda_fail(ce, "stream capture");
-    }
-    if (s.exec) {
-      cudaGraphExecUpdateResultInfo info;
-      if (cudaGraphExecUpdate(s.exec, g, &info) != cudaSuccess) {
-        cudaGetLastError();
-        cudaGraphExecDestroy(s.exec);
-        s.exec = nullptr;
-      }
-    }
-    if (s.exec == nullptr && cudaGraphInstantiate(&s.exec, g, 0) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return MYERS_E_CUDA;
-    }
-    cudaGraphDestroy(g);
-    if (cudaGraphLaunch(s.exec, s.stream) != cudaSuccess) return MYERS_E_CUDA;
-  }
+  // one graph, updated in place from the slot's previous batch.
+  if (srv->cfg.useGraphs != 0)
+    st = launch_as_graph(s.stream, &s.exec, [&] { return enqueue_batch(srv, s, plan, ne, nq, nc); });
+  else
+    st = enqueue_batch(srv, s, plan, ne, nq, nc);
   if (st != MYERS_SUCCESS) return st;
   if (cudaEventRecord(s.done, s.stream) != cudaSuccess) return MYERS_E_CUDA;
   return MYERS_SUCCESS;

@@ -74,6 +74,7 @@ _sig("myersReceive", _I32, _P)
 _sig("myersEnd", _I32, C.POINTER(_PP))
 _sig("myersSetWindowMode", _I32, _P, _I32)
 _sig("myersSetKernelPath", _I32, _P, _I32)
+_sig("myersSetGraphs", _I32, _P, _I32)
 _sig("myersSetMemoryBudget", _I32, _U64)
 _sig("myersGetDevice", _I32, _P)
 _sig("myersGetLastStatus", _I32, _P)
@@ -111,7 +112,7 @@ EXPORTED = (
     "getPEQBuffer getCandidatesBuffer getPEQInfoBuffer getResultsBuffer getMaxPEQEntries "
     "getMaxCandidates getMaxQueries initMyers sendMyersBuffer receiveMyersBuffer endMyers "
     "myersGetErrorString myersInit myersSend myersReceive myersEnd myersSetWindowMode "
-    "myersSetKernelPath myersSetMemoryBudget myersGetDevice myersGetLastStatus myersReferenceCreate "
+    "myersSetKernelPath myersSetGraphs myersSetMemoryBudget myersGetDevice myersGetLastStatus myersReferenceCreate "
     "myersReferenceLoad myersReferenceDestroy myersReferenceSize myersContextCreate myersContextDestroy "
     "myersVerifyAsync myersVerifyRangeAsync myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
     "myersPackPEQAsync myersPackReferenceAsync "
@@ -196,6 +197,10 @@ class Buffers:
     def set_path(self, path, i=None):
         for h in (self.handles if i is None else [self.handles[i]]):
             check(lib.myersSetKernelPath(h, path), "myersSetKernelPath")
+
+    def set_graphs(self, enable, i=None):
+        for h in (self.handles if i is None else [self.handles[i]]):
+            check(lib.myersSetGraphs(h, int(bool(enable))), "myersSetGraphs")
 
     def send(self, i, distance, num_entries, num_queries, num_cands):
         return check(lib.myersSend(self.handles[i], distance, num_entries, num_queries, num_cands), "myersSend")

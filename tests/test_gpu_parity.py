@@ -232,3 +232,43 @@ def test_dropin_buffers(gpu, orc, workloads, path):
         finally:
             bufs.close()
             gpu.lib.myersSetMemoryBudget(0)
+
+
+def test_dropin_graph_replay(gpu, orc, workloads):
+    """Sends replayed as CUDA graphs: consecutive sends of other sizes (graph
+    updated in place), other length mixes and kernel paths (new topology),
+    window modes and an empty send all give the results of plain stream
+    launches and the oracle's."""
+    ref, ref_size, ws = workloads
+    with tempfile.TemporaryDirectory() as tmp:
+        fn = os.path.join(tmp, "g.4bits.ref")
+        _write_ref_file(fn, ref, ref_size)
+        gpu.lib.myersSetMemoryBudget(256 << 20)
+        bufs = gpu.Buffers(fn, num_buffers=2, avg_query_size=400, cands_per_query=10)
+        try:
+            bufs.set_graphs(True, 0)
+            bufs.set_graphs(False, 1)
+            w3, w5 = ws[3], ws[5]
+            sends = []
+            for k, nq in ((3, 40), (3, 7), (5, 60), (3, 40)):
+                w = ws[k]
+                qi = w["qinfo"][:nq]
+                last = qi[-1]
+                ne = int(last["posEntry"]) + (int(last["size"]) + 127) // 128
+                sends.append((w["peq"][:ne], qi, w["cands"][w["cands"]["query"] < nq]))
+            empty = (w3["peq"][:1], w3["qinfo"][:1], w3["cands"][:0])
+            plan = [(gpu.PATH_BATCHED, gpu.WINDOW_ALIGNED, s) for s in sends] + \
+                   [(gpu.PATH_PLAIN, gpu.WINDOW_ALIGNED, s) for s in sends] + \
+                   [(gpu.PATH_BATCHED, gpu.WINDOW_EXACT, sends[2]), (gpu.PATH_BATCHED, gpu.WINDOW_ALIGNED, empty),
+                    (gpu.PATH_PLAIN, gpu.WINDOW_ALIGNED, sends[0])]
+            for path, window, (peq, qinfo, cands) in plan:
+                expect = orc.verify(peq, qinfo, cands, ref, ref_size, DIST, exact=window == gpu.WINDOW_EXACT)
+                for i in (0, 1):
+                    bufs.set_path(path, i)
+                    bufs.set_window_mode(window, i)
+                    res, st = gpu.verify_buffers(bufs, peq, qinfo, cands, DIST, buffer=i)
+                    assert st == gpu.SUCCESS
+                    assert np.array_equal(res, expect), (path, window, len(cands), i)
+        finally:
+            bufs.close()
+            gpu.lib.myersSetMemoryBudget(0)
