@@ -286,6 +286,67 @@ int myersContextFlags(myersContext_t *ctx, uint32_t *flags, int clear);
 uint32_t myersBufferLastLaunches(void *myersBuffer);
 
 /* ---------------------------------------------------------------------------
+ * Traceback of accepted candidates (no counterpart in the reference, which
+ * returns only the end column and the distance).
+ *
+ * For a candidate whose result (column c, score s) has s <= maxScore, the
+ * alignment is the path through the semi-global edit-distance matrix of its
+ * window (D[0][j] = 0, D[i][0] = i, unit costs; a query base matches a text
+ * base as in the verification, so N matches N) from (m, c+1) back to row 0
+ * that takes, at each cell, the first consistent step of: the diagonal
+ * ('=' or 'X'), the query base alone ('I'), the text base alone ('D').
+ * ------------------------------------------------------------------------- */
+
+/* Per candidate: the first window column the alignment consumes (c + 1 when
+ * it consumes none), the number of run-length ops, and the result's score
+ * and end column. numOps is MYERS_TB_NOT_TRACED for candidates above
+ * maxScore or without a result, MYERS_TB_INCONSISTENT when the result does
+ * not follow from the inputs (or a candidate's indices are out of range),
+ * and a count above maxOpsPerCandidate when the ops did not fit (the ops
+ * are then unspecified; trace again with more room). */
+typedef struct {
+    uint32_t startColumn;
+    uint32_t numOps;
+    uint32_t score;
+    uint32_t endColumn;
+} myersAlignment_t;
+
+#define MYERS_TB_NOT_TRACED 0xFFFFFFFFu
+#define MYERS_TB_INCONSISTENT 0xFFFFFFFEu
+/* ops[k] = length << 4 | code, first op first; codes as SAM's BAM encoding */
+#define MYERS_CIGAR_INS 1u
+#define MYERS_CIGAR_DEL 2u
+#define MYERS_CIGAR_EQ 7u
+#define MYERS_CIGAR_X 8u
+
+/* Work space of the traceback: ids of up to maxCandidates candidates and
+ * scratchBytes (>= 1 MiB) of device memory for the stored bit-vectors of the
+ * candidates traced in one pass (a read of 1000 bases at score 60 needs
+ * about 90 KB). */
+typedef struct myersTraceback myersTraceback_t;
+int myersTracebackCreate(myersTraceback_t **tb, uint64_t maxCandidates, uint64_t scratchBytes);
+int myersTracebackDestroy(myersTraceback_t *tb);
+
+/* Trace the candidates of a verified batch. Inputs as myersVerifyAsync plus
+ * the batch's results (d_results, device) from the same distance and window
+ * mode; outputs: d_ops (numCandidates * maxOpsPerCandidate u32; candidate
+ * k's ops at k * maxOpsPerCandidate) and d_alignments (numCandidates).
+ * Enqueued on `stream`; synchronises the stream once, after selecting the
+ * candidates to trace, to size the passes over the scratch. Not for use
+ * during stream capture. */
+int myersTraceback(myersTraceback_t *tb, const myersReference_t *ref,
+                   const qryEntry_t *d_peq, uint32_t numPEQEntries,
+                   const qryInfo_t *d_qinfo, uint32_t numQueries,
+                   const candInfo_t *d_cands, const resEntry_t *d_results, uint32_t numCandidates,
+                   float distance, int windowMode, uint32_t maxScore,
+                   uint32_t *d_ops, uint32_t maxOpsPerCandidate, myersAlignment_t *d_alignments,
+                   void *stream);
+
+/* Candidates traced by the last myersTraceback, and the passes it made. */
+uint32_t myersTracebackLastCount(const myersTraceback_t *tb);
+uint32_t myersTracebackLastChunks(const myersTraceback_t *tb);
+
+/* ---------------------------------------------------------------------------
  * Serving loop (no counterpart in the reference): requests -- one read and
  * its candidate positions -- are admitted under a device-memory budget and
  * verified in batches that form continuously: while some batches are on the

@@ -17,8 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["myers_kernels.cu", "myers_api.cu", "myers_serve.cu"]
-CUDA_HEADERS = ["myers_internal.h", os.path.join("..", "..", "include", "myers-interface.h")]
+CUDA_SOURCES = ["myers_kernels.cu", "myers_api.cu", "myers_serve.cu", "myers_traceback.cu"]
+CUDA_HEADERS = ["myers_internal.h", "myers_device.cuh", os.path.join("..", "..", "include", "myers-interface.h")]
 
 
 def _newer(target, deps):

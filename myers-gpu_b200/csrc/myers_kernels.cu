@@ -36,39 +36,9 @@
 #include <utility>
 
 #include "myers_internal.h"
+#include "myers_device.cuh"
 
 namespace myers {
-
-#define FULL_MASK 0xFFFFFFFFu
-
-__device__ __forceinline__ uint32_t d_window_bases(uint32_t m, float distance) {
-  // (uint32_t)(m * (1 + 2*distance)) in float32, no contraction.
-  float f = __fadd_rn(1.0f, __fmul_rn(2.0f, distance));
-  return (uint32_t)__fmul_rn((float)m, f);
-}
-
-__device__ __forceinline__ uint32_t d_window_words(uint32_t wb) { return wb / 8 + ((wb % 8) ? 2u : 1u); }
-
-// Reference codes 5..7 behave as A (code 0) and bit 3 is ignored, as in the
-// reference kernel's select (src-api/coreMyersGPU-CC50.cu:82-95, :170).
-__device__ __forceinline__ uint32_t sanitize_codes(uint32_t t) {
-  uint32_t c = t & 0x77777777u;
-  uint32_t bad = (c + 0x33333333u) & 0x88888888u;  // nibbles holding 5..7
-  uint32_t mask = bad - (bad >> 3);                 // 0x7 in those nibbles
-  return c & ~mask;
-}
-
-__device__ __forceinline__ uint32_t ref_load(const uint32_t* __restrict__ ref, long long idx,
-                                             unsigned long long nwords) {
-  return (idx >= 0 && (unsigned long long)idx < nwords) ? __ldg(ref + idx) : kPadWord;
-}
-
-// Word x of the query's bit vector for base c (0 outside the query).
-__device__ __forceinline__ uint32_t qword(const uint32_t* __restrict__ peq, uint32_t pos_entry,
-                                          int nw, int c, int x) {
-  return (x >= 0 && x < nw) ? __ldg(peq + (size_t)(pos_entry + (uint32_t)(x >> 2)) * 20u + c * 4 + (x & 3))
-                            : 0u;
-}
 
 // Shared-memory PEQ of one warp. Candidates of the same read share one slot
 // (the candidates of a read are adjacent in a tile), so a warp stages one

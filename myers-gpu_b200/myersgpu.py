@@ -106,6 +106,11 @@ _sig("myersShapeOf", _I32, _I32, _U32, C.POINTER(_I32), C.POINTER(_I32), C.POINT
 _sig("myersSetShapeOverride", _I32, _I32, _U32, _I32, _I32)
 _sig("myersTunedShapes", _I32, _I32)
 _sig("myersProbeIntPeak", _I32, C.POINTER(C.c_double), _I32)
+_sig("myersTracebackCreate", _I32, _PP, _U64, _U64)
+_sig("myersTracebackDestroy", _I32, _P)
+_sig("myersTraceback", _I32, _P, _P, _P, _U32, _P, _U32, _P, _P, _U32, _F, _I32, _U32, _P, _U32, _P, _P)
+_sig("myersTracebackLastCount", _U32, _P)
+_sig("myersTracebackLastChunks", _U32, _P)
 
 # Every symbol the C header declares (the CPU tests check the exports).
 EXPORTED = (
@@ -118,8 +123,13 @@ EXPORTED = (
     "myersPackPEQAsync myersPackReferenceAsync "
     "myersBufferLastLaunches myersNumVariants myersVariantWords myersVariantIsMulti myersShapeOf "
     "myersSetShapeOverride myersTunedShapes myersProbeIntPeak myersServerCreate myersServerSubmit myersServerPoll myersServerWait "
-    "myersServerStats myersServerDestroy myersServerReplay"
+    "myersServerStats myersServerDestroy myersServerReplay myersTracebackCreate myersTracebackDestroy "
+    "myersTraceback myersTracebackLastCount myersTracebackLastChunks"
 ).split()
+
+ALN = np.dtype([("start_column", "<u4"), ("num_ops", "<u4"), ("score", "<u4"), ("end_column", "<u4")])
+TB_NOT_TRACED = 0xFFFFFFFF
+TB_INCONSISTENT = 0xFFFFFFFE
 
 
 def error_string(status):
@@ -282,6 +292,60 @@ class Context:
         if self.h:
             lib.myersContextDestroy(self.h)
             self.h = C.c_void_p()
+
+
+class Traceback:
+    """Work space of myersTraceback: ids of up to max_candidates candidates
+    and scratch_bytes of device memory for the stored band of each traced
+    candidate."""
+
+    def __init__(self, max_candidates, scratch_bytes=1 << 30):
+        self.h = C.c_void_p()
+        check(lib.myersTracebackCreate(C.byref(self.h), max_candidates, scratch_bytes), "myersTracebackCreate")
+
+    def run(self, ref, d_peq, n_entries, d_qinfo, n_queries, d_cands, d_results, n_cands, distance, max_score,
+            d_ops, max_ops, d_alns, window=WINDOW_ALIGNED, stream=0):
+        """Enqueue on `stream`; pointers are device addresses. Returns the
+        number of candidates traced."""
+        check(lib.myersTraceback(self.h, ref.h, d_peq, n_entries, d_qinfo, n_queries, d_cands, d_results, n_cands,
+                                 distance, window, max_score, d_ops, max_ops, d_alns, stream), "myersTraceback")
+        return lib.myersTracebackLastCount(self.h)
+
+    def chunks(self):
+        return lib.myersTracebackLastChunks(self.h)
+
+    def close(self):
+        if self.h:
+            lib.myersTracebackDestroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def traceback_torch(tb, ref, peq, qinfo, cands, results, distance, max_score, max_ops, window=WINDOW_ALIGNED):
+    """Trace numpy inputs (results from a verification of the same inputs)
+    on the current torch stream; returns (ALN records, ops (n, max_ops))."""
+    import torch
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1)).cuda()
+
+    n = len(cands)
+    d_peq, d_qi, d_c, d_r = dev(peq), dev(qinfo), dev(cands), dev(results)
+    d_ops = torch.zeros(max(1, n) * max_ops, dtype=torch.int32, device="cuda")
+    d_aln = torch.zeros(max(1, n) * 16, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    tb.run(ref, d_peq.data_ptr(), len(peq), d_qi.data_ptr(), len(qinfo), d_c.data_ptr(), d_r.data_ptr(), n,
+           distance, max_score, d_ops.data_ptr(), max_ops, d_aln.data_ptr(), window=window,
+           stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    aln = d_aln.cpu().numpy()[: n * 16].view(ALN)
+    ops = d_ops.cpu().numpy().view(np.uint32)[: n * max_ops].reshape(n, max_ops)
+    return aln, ops
 
 
 def verify_torch(ctx, ref, peq, qinfo, cands, distance, window=WINDOW_ALIGNED, path=PATH_PLAIN, min_size=0,

@@ -233,3 +233,137 @@ void orc_pack_peq(const uint8_t *read, uint32_t m, orc_peq_t *entries)
         entries[i / 128].bitmap[c][(i % 128) / 32] |= 1u << (i % 32);
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * Traceback of an accepted candidate. Not in the reference: the reference
+ * returns only (column, score). This is the checker of the GPU traceback and
+ * defines its result:
+ *
+ *   For a candidate whose result (column c, score s) has s <= max_score, the
+ *   alignment is the path through the semi-global edit-distance matrix
+ *   (D[0][j] = 0, D[i][0] = i, unit costs; query row i matches text column j
+ *   iff PEQ[code of text j] has bit i-1, so N matches N) from (m, c+1) back
+ *   to row 0, choosing at each cell, in this order: the diagonal
+ *   (D[i-1][j-1] + mismatch == D[i][j]; '=' or 'X'), the query base alone
+ *   (D[i-1][j] + 1 == D[i][j]; 'I'), the text base alone ('D'). Columns are
+ *   window columns as in the verification (aligned or exact window).
+ *
+ * Record: start column (first text column consumed; c+1 when none), number
+ * of run-length ops, score, end column. ops[k] = length << 4 | code with the
+ * SAM codes '=' 7, 'X' 8, 'I' 1, 'D' 2, first op first. numOps is
+ * ORC_TB_NOT_TRACED when s > max_score or the candidate has no result,
+ * ORC_TB_INCONSISTENT when (c, s) is not the inputs' result at c, and a
+ * count above max_ops when the ops did not fit (ops then unspecified).
+ * ------------------------------------------------------------------------- */
+#define ORC_TB_NOT_TRACED 0xFFFFFFFFu
+#define ORC_TB_INCONSISTENT 0xFFFFFFFEu
+
+typedef struct { uint32_t start_column; uint32_t num_ops; uint32_t score; uint32_t end_column; } orc_aln_t;
+
+static inline uint32_t text_code(const uint32_t *ref, uint64_t ref_words, uint64_t base)
+{
+    return code_of(ref_word(ref, ref_words, base / 8) >> (4 * (base % 8)));
+}
+
+static inline int peq_bit(const orc_peq_t *peq, uint32_t pos_entry, uint32_t code, uint32_t row0)
+{
+    return (peq[pos_entry + row0 / 128].bitmap[code][(row0 % 128) / 32] >> (row0 % 32)) & 1u;
+}
+
+static void push_op(uint32_t *ops, uint32_t max_ops, uint32_t *n, uint32_t *cur, uint32_t *len, uint32_t op)
+{
+    if (*len && *cur == op) { ++*len; return; }
+    if (*len) {
+        if (*n < max_ops) ops[*n] = (*len << 4) | *cur;
+        ++*n;
+    }
+    *cur = op;
+    *len = 1;
+}
+
+void orc_traceback_one(const orc_peq_t *peq, const uint32_t *ref, uint64_t ref_words, uint64_t ref_size,
+                       uint32_t pos_entry, uint32_t m, uint64_t pos, float distance, int exact,
+                       orc_res_t res, uint32_t max_score, uint32_t *ops, uint32_t max_ops, orc_aln_t *aln)
+{
+    aln->score = res.score;
+    aln->end_column = res.column;
+    aln->start_column = ORC_TB_NOT_TRACED;
+    aln->num_ops = ORC_TB_NOT_TRACED;
+    if (res.score == ORC_NO_RESULT || res.score > max_score) return;
+    aln->num_ops = ORC_TB_INCONSISTENT;
+    const uint32_t W = orc_window_bases(m, distance);
+    if (!(pos < ref_size && ref_size - pos > W)) return;
+    const uint64_t ncols = exact ? W : 8ull * orc_window_words(W);
+    const uint64_t start = exact ? pos : (pos / 8) * 8;
+    const uint64_t c1 = (uint64_t)res.column + 1;  /* 1-based end column */
+    if (c1 > ncols) return;
+    /* The path consumes at most m + s text bases, so it stays in columns
+     * >= a0; earlier columns are computed but not kept. */
+    const uint64_t a0 = c1 > (uint64_t)m + res.score ? c1 - m - res.score : 0;
+    const uint64_t kept = c1 - a0 + 1;
+    uint16_t *D = (uint16_t *)malloc(sizeof(uint16_t) * (m + 1) * kept);
+    uint16_t *col = (uint16_t *)malloc(sizeof(uint16_t) * (m + 1) * 2);
+    if (!D || !col) { free(D); free(col); return; }
+    uint16_t *prev = col, *cur = col + (m + 1);
+    for (uint32_t i = 0; i <= m; ++i) prev[i] = (uint16_t)i;
+    if (a0 == 0) memcpy(D, prev, sizeof(uint16_t) * (m + 1));
+    for (uint64_t j = 1; j <= c1; ++j) {
+        const uint32_t t = text_code(ref, ref_words, start + j - 1);
+        cur[0] = 0;
+        for (uint32_t i = 1; i <= m; ++i) {
+            uint32_t d = prev[i - 1] + (peq_bit(peq, pos_entry, t, i - 1) ? 0u : 1u);
+            uint32_t u = cur[i - 1] + 1u, l = prev[i] + 1u;
+            if (u < d) d = u;
+            if (l < d) d = l;
+            cur[i] = (uint16_t)d;
+        }
+        if (j >= a0) memcpy(D + (j - a0) * (m + 1), cur, sizeof(uint16_t) * (m + 1));
+        uint16_t *x = prev; prev = cur; cur = x;
+    }
+    if (D[(c1 - a0) * (m + 1) + m] != res.score) { free(D); free(col); return; }
+#define DV(i, j) ((uint32_t)D[((j) - a0) * (m + 1) + (i)])
+    uint32_t n = 0, cur_op = 0, len = 0;
+    /* ops are produced last first; reversed below */
+    uint32_t *rev = (uint32_t *)malloc(sizeof(uint32_t) * (m + c1 + 1));
+    uint32_t i = m;
+    uint64_t j = c1;
+    while (i > 0) {
+        uint32_t op;
+        if (j == 0 || j <= a0) {
+            /* j <= a0 only when a0 == 0 (the path never leaves columns >= a0) */
+            op = 1; --i;
+        } else {
+            const uint32_t t = text_code(ref, ref_words, start + j - 1);
+            const int match = peq_bit(peq, pos_entry, t, i - 1);
+            if (DV(i - 1, j - 1) + (match ? 0u : 1u) == DV(i, j)) { op = match ? 7u : 8u; --i; --j; }
+            else if (DV(i - 1, j) + 1u == DV(i, j)) { op = 1; --i; }
+            else { op = 2; --j; }
+        }
+        push_op(rev, m + (uint32_t)c1 + 1, &n, &cur_op, &len, op);
+    }
+#undef DV
+    if (len) rev[n++] = (len << 4) | cur_op;
+    aln->start_column = (uint32_t)j;
+    aln->num_ops = n;
+    if (n <= max_ops)
+        for (uint32_t k = 0; k < n; ++k) ops[k] = rev[n - 1 - k];
+    free(rev);
+    free(D);
+    free(col);
+}
+
+void orc_traceback(const orc_peq_t *peq, const orc_qinfo_t *qinfo, const orc_cand_t *cands,
+                   const orc_res_t *res, uint64_t num_cands, const uint32_t *ref, uint64_t ref_words,
+                   uint64_t ref_size, float distance, int exact, uint32_t max_score, uint32_t *ops,
+                   uint32_t max_ops, orc_aln_t *aln, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#endif
+    for (int64_t k = 0; k < (int64_t)num_cands; ++k) {
+        const orc_qinfo_t q = qinfo[cands[k].query];
+        orc_traceback_one(peq, ref, ref_words, ref_size, q.posEntry, q.size, cands[k].position, distance, exact,
+                          res[k], max_score, ops + (uint64_t)k * max_ops, max_ops, &aln[k]);
+    }
+}

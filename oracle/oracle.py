@@ -44,6 +44,15 @@ _orc.orc_pack_reference.restype = None
 _orc.orc_pack_reference.argtypes = [C.c_char_p, C.c_uint64, C.c_void_p]
 _orc.orc_pack_peq.restype = None
 _orc.orc_pack_peq.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p]
+_orc.orc_traceback.restype = None
+_orc.orc_traceback.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                               C.c_uint64, C.c_float, C.c_int, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                               C.c_int]
+
+ALN = np.dtype([("start_column", "<u4"), ("num_ops", "<u4"), ("score", "<u4"), ("end_column", "<u4")])
+TB_NOT_TRACED = 0xFFFFFFFF
+TB_INCONSISTENT = 0xFFFFFFFE
+OP_CODES = {7: "=", 8: "X", 1: "I", 2: "D"}
 
 
 def window_bases(m, distance):
@@ -60,6 +69,29 @@ def verify(peq, qinfo, cands, ref_words, ref_size, distance, exact=False, nthrea
     _orc.orc_verify(peq.ctypes.data, qinfo.ctypes.data, cands.ctypes.data, len(cands), ref_words.ctypes.data,
                     ref_words.size, ref_size, distance, int(exact), res.ctypes.data, nthreads)
     return res
+
+
+def traceback(peq, qinfo, cands, results, ref_words, ref_size, distance, max_score, max_ops, exact=False,
+              nthreads=0):
+    """Alignments of the candidates whose score is <= max_score: returns
+    (records of ALN, ops as a (len(cands), max_ops) u32 array; row k holds
+    num_ops[k] run-length ops, length << 4 | SAM code)."""
+    peq = np.ascontiguousarray(peq)
+    qinfo = np.ascontiguousarray(qinfo)
+    cands = np.ascontiguousarray(cands)
+    results = np.ascontiguousarray(results)
+    ref_words = np.ascontiguousarray(ref_words, dtype=np.uint32)
+    aln = np.empty(len(cands), dtype=ALN)
+    ops = np.zeros((len(cands), max(1, max_ops)), dtype=np.uint32)
+    _orc.orc_traceback(peq.ctypes.data, qinfo.ctypes.data, cands.ctypes.data, results.ctypes.data, len(cands),
+                       ref_words.ctypes.data, ref_words.size, ref_size, distance, int(exact), max_score,
+                       ops.ctypes.data, max_ops, aln.ctypes.data, nthreads)
+    return aln, ops
+
+
+def cigar(ops, n):
+    """SAM-style string of the first n run-length ops."""
+    return "".join(f"{int(o) >> 4}{OP_CODES[int(o) & 15]}" for o in ops[:n])
 
 
 def pack_reference(ascii_bases):

@@ -138,3 +138,86 @@ def test_synth_thread_independent(mg):
         outs.add(subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
                                 check=True).stdout)
     assert len(outs) == 1
+
+
+def _dp_traceback(qc, tc, end_col):
+    """Pure-Python DP and traceback with the stated step order (diagonal,
+    query base alone, text base alone) from (m, end_col + 1). Returns
+    (start column, ops as (code, length) runs)."""
+    m, n = len(qc), end_col + 1
+    D = [[0] * (n + 1) for _ in range(m + 1)]
+    for i in range(1, m + 1):
+        D[i][0] = i
+        for j in range(1, n + 1):
+            D[i][j] = min(D[i - 1][j - 1] + (qc[i - 1] != tc[j - 1]), D[i - 1][j] + 1, D[i][j - 1] + 1)
+    i, j, rev = m, n, []
+    while i > 0:
+        if j > 0 and D[i - 1][j - 1] + (qc[i - 1] != tc[j - 1]) == D[i][j]:
+            rev.append("=" if qc[i - 1] == tc[j - 1] else "X")
+            i, j = i - 1, j - 1
+        elif D[i - 1][j] + 1 == D[i][j]:
+            rev.append("I")
+            i -= 1
+        else:
+            rev.append("D")
+            j -= 1
+    runs = []
+    for op in reversed(rev):
+        if runs and runs[-1][0] == op:
+            runs[-1][1] += 1
+        else:
+            runs.append([op, 1])
+    return j, [(o, k) for o, k in runs]
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_oracle_traceback_matches_textbook(orc, mg, exact):
+    """The oracle's traceback (the definition the GPU path is checked
+    against) equals an independent pure-Python DP traceback, and every
+    alignment is consistent: query bases = m, text bases = end - start + 1,
+    edit cost = score."""
+    rng = np.random.default_rng(11 + exact)
+    ref_size = 4000
+    ascii_ref = bytes(rng.choice(list(b"ACGTN"), size=ref_size, p=[0.24, 0.24, 0.24, 0.24, 0.04]).astype(np.uint8))
+    words = orc.pack_reference(ascii_ref)
+    peq, qinfo, cands, reads = [], [], [], []
+    entry = 0
+    for q in range(10):
+        m = int(rng.integers(1, 60))
+        read = bytes(rng.choice(list(b"ACGTN"), size=m).astype(np.uint8))
+        reads.append(["ACGTN".index(chr(b)) for b in read])
+        peq.append(orc.pack_peq(read).reshape(-1, 20))
+        qinfo.append((entry, m))
+        entry += (m + 127) // 128
+        W = orc.window_bases(m, 0.2)
+        for _ in range(4):
+            cands.append((q, int(rng.integers(0, ref_size - W - 20))))
+    peq = np.concatenate(peq).ravel().view(mg.QRY_ENTRY)
+    qinfo = np.array(qinfo, dtype=np.uint32).view(mg.QINFO).ravel()
+    c = np.zeros(len(cands), dtype=mg.CAND)
+    c["query"] = [x[0] for x in cands]
+    c["position"] = [x[1] for x in cands]
+    res = orc.verify(peq, qinfo, c, words, ref_size, 0.2, exact=exact)
+    aln, ops = orc.traceback(peq, qinfo, c, res, words, ref_size, 0.2, 10 ** 6, 256, exact=exact)
+    names = {7: "=", 8: "X", 1: "I", 2: "D"}
+    for k, (q, pos) in enumerate(cands):
+        m = len(reads[q])
+        W = orc.window_bases(m, 0.2)
+        start = pos if exact else pos - pos % 8
+        ncols = W if exact else 8 * (W // 8 + (2 if W % 8 else 1))
+        tc = _codes(words, start, ncols)
+        tc = [0 if t > 4 else t for t in tc]
+        a0, runs = _dp_traceback(reads[q], tc, int(res["column"][k]))
+        got = [(names[int(o) & 15], int(o) >> 4) for o in ops[k, : aln["num_ops"][k]]]
+        assert (int(aln["start_column"][k]), got) == (a0, runs)
+        n_q = sum(n for o, n in got if o in "=XI")
+        n_t = sum(n for o, n in got if o in "=XD")
+        cost = sum(n for o, n in got if o in "XID")
+        assert n_q == m and n_t == int(res["column"][k]) - a0 + 1 and cost == int(res["score"][k])
+    # a bound below every score traces nothing; a wrong score is caught
+    aln0, _ = orc.traceback(peq, qinfo, c, res, words, ref_size, 0.2, 0, 16, exact=exact)
+    assert ((aln0["num_ops"] == orc.TB_NOT_TRACED) | (res["score"] == 0)).all()
+    bad = res.copy()
+    bad["score"] += 1
+    aln1, _ = orc.traceback(peq, qinfo, c, bad, words, ref_size, 0.2, 10 ** 6, 16, exact=exact)
+    assert (aln1["num_ops"] == orc.TB_INCONSISTENT).all()
