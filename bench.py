@@ -66,6 +66,10 @@ def parse_args():
     ap.add_argument("--lane-words", type=int, default=12, help="serving: words per lane of the latency shapes")
     ap.add_argument("--slots", type=int, default=4, help="serving: batches in flight")
     ap.add_argument("--no-graphs", action="store_true", help="serving: launch batches without CUDA graphs")
+    ap.add_argument("--traceback", action="store_true",
+                    help="time the traceback of the workload's candidates within --tb-bound x m")
+    ap.add_argument("--tb-bound", type=float, default=0.2, help="traceback: score bound as a fraction of m")
+    ap.add_argument("--tb-scratch-gb", type=float, default=16.0, help="traceback: scratch for the stored bands")
     return ap.parse_args()
 
 
@@ -569,10 +573,116 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_traceback(args):
+    """Traceback of the candidates whose score is within the bound: one step
+    = one myersTraceback call over the verified batch (selection, the
+    band-storing forward pass and the walk), inputs and results resident."""
+    import torch
+
+    import myersgpu as mg
+    torch.cuda.set_device(0)
+    k = args.workload
+    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0)
+    n = len(w["cands"])
+    m_of = w["qinfo"]["size"][w["cands"]["query"]].astype(np.int64)
+    max_score = int(args.tb_bound * int(m_of.max()))
+    ref = mg.Reference(ref_words, ref_size)
+    ctx = mg.Context(n)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to("cuda")
+
+    d_peq, d_qi, d_c = dev(w["peq"]), dev(w["qinfo"]), dev(w["cands"])
+    d_res = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    ctx.verify(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(), n, DIST,
+               d_res.data_ptr(), path=mg.PATH_BATCHED, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    res = d_res.cpu().numpy().view(mg.RES)
+    max_ops = 256  # runs per candidate: about 2 per edit of a traced alignment, plus one
+    d_ops = torch.empty(n * max_ops, dtype=torch.int32, device="cuda")
+    d_aln = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
+    tb = mg.Traceback(n, int(args.tb_scratch_gb * (1 << 30)))
+
+    def step():
+        return tb.run(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(),
+                      d_res.data_ptr(), n, DIST, max_score, d_ops.data_ptr(), max_ops, d_aln.data_ptr(),
+                      stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        traced = step()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    clocks = ClockSampler(0)
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        traced = step()
+        b.record(stream)
+        clocks.poke()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) / 1e3)
+    clk = clocks.stop()
+    del flush
+    t = float(np.mean(times))
+    aln = d_aln.cpu().numpy().view(mg.ALN)
+    ops = d_ops.cpu().numpy().view(np.uint32).reshape(n, max_ops)
+    sel = (res["score"] != mg.NO_RESULT) & (res["score"] <= max_score)
+    # work of the forward pass: ceil(m/32) words x (end column + 1) columns per traced candidate
+    ws = float((np.ceil(m_of[sel] / 32.0) * (res["column"][sel].astype(np.float64) + 1)).sum())
+    peak = mg.probe_int_peak(4000)
+    achieved = ws * OPS_PER_WORD_STEP / t
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    idx = np.nonzero(sel)[0]
+    pick = np.random.default_rng(5).choice(idx, size=min(300, len(idx)), replace=False)
+    e_aln, e_ops = orc.traceback(w["peq"], w["qinfo"], w["cands"][pick], res[pick], ref_words, ref_size, DIST,
+                                 max_score, max_ops)
+    # records compared whole; ops where they fit (else both leave them unspecified)
+    ok = np.array_equal(aln[pick].view(np.uint32), e_aln.view(np.uint32)) and all(
+        np.array_equal(ops[i, :e_aln["num_ops"][j]], e_ops[j, :e_aln["num_ops"][j]])
+        for j, i in enumerate(pick) if e_aln["num_ops"][j] <= max_ops)
+    overflow = int((aln["num_ops"][sel] > max_ops).sum())
+    # CPU baseline: the oracle's DP traceback on a bounded sample, all host threads
+    cores = host_threads()
+    sample = idx[: max(1, min(len(idx), 4000))]
+    t0 = time.perf_counter()
+    orc.traceback(w["peq"], w["qinfo"], w["cands"][sample], res[sample], ref_words, ref_size, DIST, max_score,
+                  max_ops, nthreads=cores)
+    cpu_s = time.perf_counter() - t0
+    chunks = int(tb.chunks())
+    ctx.close()
+    ref.close()
+    tb.close()
+    line = {
+        "metric": "alignments/s", "value": traced / t, "unit": "alignments/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+        "config": {"workload": "traceback of " + WORKLOAD_NAMES[k], "traced": int(traced), "candidates": n,
+                   "max_score": max_score, "max_ops": max_ops, "scratch_gib": args.tb_scratch_gb,
+                   "l2": "L2 flushed before every timed step (256 MiB write, untimed)"},
+        "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": "whole call (selection, host read of the count, forward pass, walk) against the "
+                             "forward pass's word-steps x 11"},
+        "cpu_baseline": {"value": len(sample) / cpu_s, "unit": "alignments/s", "cores": cores, "kind": "port",
+                         "sample": f"{len(sample)} traced candidates, the oracle's O(mn) DP traceback"},
+        "parity_sample": {"candidates": int(len(pick)), "bit_exact": bool(ok)},
+        "ops_overflow": overflow,
+        "clocks": clk, "gpu_launches": 1 + 2 * chunks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.traceback:
+        run_traceback(args)
     elif args.workload == 5:
         run_serving(args)
     else:
