@@ -321,8 +321,12 @@ typedef struct {
 
 /* Work space of the traceback: ids of up to maxCandidates candidates and
  * scratchBytes (>= 1 MiB) of device memory for the stored bit-vectors of the
- * candidates traced in one pass (a read of 1000 bases at score 60 needs
- * about 90 KB). */
+ * traced candidates. Passes alternate between the two halves of the scratch
+ * (one pass's walk overlaps the next pass's recomputation), so half of it
+ * must hold the band of the widest traced candidate, else myersTraceback
+ * returns MYERS_E_CAPACITY: a read of 1000 bases needs about 90 KB at score
+ * 60 and about 900 KB at score 600. Calls on one traceback object must be
+ * ordered (one stream, or synchronised). */
 typedef struct myersTraceback myersTraceback_t;
 int myersTracebackCreate(myersTraceback_t **tb, uint64_t maxCandidates, uint64_t scratchBytes);
 int myersTracebackDestroy(myersTraceback_t *tb);

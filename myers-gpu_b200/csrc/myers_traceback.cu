@@ -9,19 +9,28 @@
 // ('I'), the text base alone ('D') that is consistent with the matrix.
 //
 // Two passes per chunk of traced candidates:
-//  * k_tb_forward: one candidate per warp, its rows spread over L lanes of W
-//    words (the systolic layout of the multi-lane verification shapes: lane
-//    l processes column t - l at step t, taking the horizontal delta of its
-//    bottom row from lane l-1 through a shuffle). It recomputes the window's
-//    columns 1..c+1 and stores, for each column, the words of the diagonal
-//    band the path can use: Pv/Mv (vertical deltas) and Ph/Mh (horizontal
-//    deltas into the column). A path of cost s from (0, a) to (m, c+1) has
-//    j - i within s of (c+1) - m at every cell, and consumes at most m + s
-//    text bases, so columns before c+1-m-s and rows outside that band are
-//    never read back.
-//  * k_tb_walk: one thread per candidate walks back with three bit lookups
-//    per step: the diagonal is consistent iff h(i,j) + v(i,j-1) equals the
-//    mismatch cost, the query base alone iff v(i,j) = +1.
+//  * k_tb_forward: a candidate's rows are spread over L lanes of W words (W
+//    >= 8, one choice per call), a warp holding 32/S candidates in segments
+//    of S lanes. Lanes run as a systolic pipeline (lane r processes column
+//    t - r at step t, taking the horizontal delta of its bottom row from
+//    lane r-1 through a shuffle). The pass recomputes the window's columns
+//    1..c+1 and stores, for each column, the words of the diagonal band the
+//    path can use: Pv/Mv (vertical deltas) and Ph/Mh (horizontal deltas into
+//    the column). A path of cost s from (0, a) to (m, c+1) has j - i within
+//    s of (c+1) - m at every cell, and consumes at most m + s text bases, so
+//    columns before c+1-m-s and rows outside that band are never read back.
+//  * k_tb_walk: one thread per candidate walks back with bit lookups: the
+//    diagonal is consistent iff h(i,j) + v(i,j-1) equals the mismatch cost,
+//    the query base alone iff v(i,j) = +1. The columns to the left are
+//    fetched four ahead, the PEQ words once per 32 rows and the text once
+//    per 8 columns, so a step rarely waits on a load it has just issued.
+// Each traced candidate reserves its own band store (256-byte units) when it
+// is selected: one 64-bit atomic per warp takes both its place in the list
+// and its offset, so offsets rise with list order. A chunk is the range of
+// the list whose offsets fall in one window of half the scratch (found by
+// binary search); chunks alternate between the two halves, the walk of one
+// (latency-bound) running on a second stream beside the forward pass of the
+// next (ALU-bound).
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -38,10 +47,15 @@ static constexpr uint32_t kTbNotTraced = 0xFFFFFFFFu;
 static constexpr uint32_t kTbInconsistent = 0xFFFFFFFEu;
 static constexpr uint32_t kOpEq = 7, kOpX = 8, kOpI = 1, kOpD = 2;  // SAM codes
 
+// packed = traced count << 36 | their band stores in 256-byte units
+static constexpr unsigned kTbUnitShift = 8;
+static constexpr unsigned kTbCountShift = 36;
+static constexpr unsigned long long kTbUnitMask = (1ull << kTbCountShift) - 1ull;
+
 struct TbState {
-  unsigned int count;               // candidates to trace
-  unsigned int max_wl;              // widest words-per-lane among them
-  unsigned long long max_slot;      // largest band store (bytes)
+  unsigned long long packed;
+  unsigned int max_words;  // longest query among them (32-bit words)
+  unsigned int max_units;  // largest band store (256-byte units), for any words per lane
 };
 
 struct TbArgs {
@@ -59,26 +73,35 @@ struct TbArgs {
   uint32_t* ops;
   uint32_t max_ops;
   uint4* alns;  // {startColumn, numOps, score, endColumn}
-  uint32_t* ids;
+  const uint32_t* ids;             // traced candidates, in reservation order
+  const unsigned long long* offs;  // their band stores' offsets (units), rising
+  uint32_t count;                  // traced candidates
   TbState* st;
-  unsigned char* scratch;
-  unsigned long long slot_bytes;
+  unsigned char* scratch;          // this chunk's half
+  unsigned long long unit_lo, unit_hi;  // this chunk: offsets in [unit_lo, unit_hi)
+  uint32_t wl;   // words per lane of this call
+  uint32_t seg;  // lanes per candidate segment (power of two)
 };
 
 // Geometry of one traced candidate (identical in all three kernels).
 struct TbGeom {
   uint32_t m, pos_entry, s, c1;  // c1 = end column + 1 (1-based)
-  uint32_t wl, L, tw, p;         // words per lane, lanes, L*wl, padding rows
+  uint32_t L, tw, p;             // lanes, L*wl words, padding rows
   uint32_t a0, B;                // first kept column, band words per column
   int off;                       // c1 - m: the path's final diagonal
   unsigned long long start;      // window start (bases)
 };
 
-__host__ __device__ __forceinline__ uint32_t tb_words_per_lane(uint32_t words) {
-  uint32_t wl = 1;
+// Words per lane for queries of up to `words` words: 8 up to 256 words
+// (8192 bases), then doubling, so that a query takes at most 32 lanes.
+static inline uint32_t tb_words_per_lane(uint32_t words) {
+  uint32_t wl = 8;
   while (32u * wl < words) wl <<= 1;
   return wl;
 }
+
+// Band words per column for score s, before the cap at the query's words.
+__device__ __forceinline__ uint32_t tb_band_words(uint32_t s) { return (2u * s + 3u + 31u) / 32u + 1u; }
 
 // Band: the first stored word of column j1 (1-based).
 __device__ __forceinline__ uint32_t tb_xlo(const TbGeom& g, uint32_t j1) {
@@ -89,8 +112,9 @@ __device__ __forceinline__ uint32_t tb_xlo(const TbGeom& g, uint32_t j1) {
 }
 
 // Returns 0 and fills g when the candidate is traced; else the numOps code
-// of its record (not traced / inconsistent), or 1 for an empty query.
-__device__ __forceinline__ uint32_t tb_setup(const TbArgs& a, uint32_t id, uint2 res, TbGeom& g) {
+// of its record (not traced / inconsistent), or 1 for an empty query. With
+// wl = 0 the lane layout (L, tw, p, B) is left out (the selection pass).
+__device__ __forceinline__ uint32_t tb_setup(const TbArgs& a, uint32_t id, uint2 res, uint32_t wl, TbGeom& g) {
   if (res.y == kNoResult || res.y > a.max_score) return kTbNotTraced;
   const Cand cd = a.cands[id];
   if (cd.query >= a.num_queries) return kTbInconsistent;
@@ -106,49 +130,68 @@ __device__ __forceinline__ uint32_t tb_setup(const TbArgs& a, uint32_t id, uint2
   if (g.c1 > n || n > kMaxColumns || g.m > kMaxWords * 32u) return kTbInconsistent;
   if (g.m == 0) return (res.x == 0 && res.y == 0) ? 1u : kTbInconsistent;
   if (g.s > g.m) return kTbInconsistent;  // D[m][j] <= m for every column
-  const uint32_t words = (g.m + 31u) >> 5;
-  g.wl = tb_words_per_lane(words);
-  g.L = (words + g.wl - 1u) / g.wl;
-  g.tw = g.L * g.wl;
-  g.p = 32u * g.tw - g.m;
   g.off = (int)g.c1 - (int)g.m;
   g.a0 = g.c1 > g.m + g.s ? g.c1 - g.m - g.s : 0u;
-  const uint32_t b = (2u * g.s + 3u + 31u) / 32u + 1u;
-  g.B = b < g.tw ? b : g.tw;
   g.start = a.exact ? cd.position : (cd.position & ~7ull);
+  if (wl) {
+    const uint32_t words = (g.m + 31u) >> 5;
+    g.L = (words + wl - 1u) / wl;
+    g.tw = g.L * wl;
+    g.p = 32u * g.tw - g.m;
+    const uint32_t b = tb_band_words(g.s);
+    g.B = b < g.tw ? b : g.tw;
+  }
   return 0u;
 }
 
-__device__ __forceinline__ unsigned long long tb_slot_bytes(const TbGeom& g) {
-  return (unsigned long long)(g.c1 - g.a0 + 1u) * g.B * 16ull;
+// Bytes of a candidate's band store for any words per lane (the cap uses
+// the largest possible L*wl, words + 31).
+__device__ __forceinline__ unsigned long long tb_slot_bound(const TbGeom& g) {
+  const uint32_t words = (g.m + 31u) >> 5, b = tb_band_words(g.s);
+  const uint32_t B = b < words + 31u ? b : words + 31u;
+  return (unsigned long long)(g.c1 - g.a0 + 1u) * B * 16ull;
 }
 
 // Pick the candidates to trace; write the records of the others.
-__global__ void k_tb_select(TbArgs a) {
+__global__ void k_tb_select(TbArgs a, uint32_t* ids, unsigned long long* offs) {
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t base = blockIdx.x * blockDim.x; base < a.num_cands; base += gridDim.x * blockDim.x) {
     const uint32_t id = base + threadIdx.x;
     bool traced = false;
+    uint32_t units = 0;
     TbGeom g;
     if (id < a.num_cands) {
       const uint2 res = a.results[id];
-      const uint32_t why = tb_setup(a, id, res, g);
+      const uint32_t why = tb_setup(a, id, res, 0u, g);
       uint4 rec = make_uint4(kTbNotTraced, why, res.y, res.x);
       if (why == 1u) rec = make_uint4(res.x + 1u, 0u, res.y, res.x);  // empty query: empty alignment
       if (why == 0u) {
         traced = true;
         rec.y = 0u;
-        atomicMax(&a.st->max_wl, g.wl);
-        atomicMax(&a.st->max_slot, tb_slot_bytes(g));
+        units = (uint32_t)((tb_slot_bound(g) + (1ull << kTbUnitShift) - 1ull) >> kTbUnitShift);
+        atomicMax(&a.st->max_words, (g.m + 31u) >> 5);
+        atomicMax(&a.st->max_units, units);
       }
       a.alns[id] = rec;
     }
-    // warp-aggregated append of the traced ids
+    // warp-aggregated append: list places and band offsets in one atomic
     const uint32_t mask = __ballot_sync(FULL_MASK, traced);
-    uint32_t first = 0;
-    if (lane == 0 && mask) first = atomicAdd(&a.st->count, (unsigned)__popc(mask));
-    first = __shfl_sync(FULL_MASK, first, 0);
-    if (traced) a.ids[first + __popc(mask & ((1u << lane) - 1u))] = id;
+    unsigned long long incl = units;  // inclusive prefix of the units over the warp
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned long long v = __shfl_up_sync(FULL_MASK, incl, d);
+      if ((int)lane >= d) incl += v;
+    }
+    const unsigned long long total = __shfl_sync(FULL_MASK, incl, 31);
+    unsigned long long old = 0;
+    if (lane == 0 && mask)
+      old = atomicAdd(&a.st->packed, ((unsigned long long)__popc(mask) << kTbCountShift) + total);
+    old = __shfl_sync(FULL_MASK, old, 0);
+    if (traced) {
+      const uint32_t pos = (uint32_t)(old >> kTbCountShift) + __popc(mask & ((1u << lane) - 1u));
+      ids[pos] = id;
+      offs[pos] = (old & kTbUnitMask) + incl - units;
+    }
   }
 }
 
@@ -160,20 +203,22 @@ __device__ __forceinline__ int tb_column(const uint32_t* __restrict__ eq, uint32
                                          int hin, uint32_t (&ph)[W], uint32_t (&mh)[W]) {
   uint32_t e[W], t[W], s[W];
 #pragma unroll
-  for (int k = 0; k < W; ++k) e[k] = eq[k];
+  for (int k = 0; k < W; k += 4) {
+    const uint4 v = *reinterpret_cast<const uint4*>(eq + k);
+    e[k] = v.x;
+    e[k + 1] = v.y;
+    e[k + 2] = v.z;
+    e[k + 3] = v.w;
+  }
   const uint32_t e0 = e[0] | (hin < 0 ? 1u : 0u);
   t[0] = e0 & Pv[0];
 #pragma unroll
   for (int k = 1; k < W; ++k) t[k] = e[k] & Pv[k];
-  // multi-word add t + Pv
-  uint32_t carry = 0;
+  // multi-word add t + Pv as one carry chain
+  asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(t[0]), "r"(Pv[0]));
 #pragma unroll
-  for (int k = 0; k < W; ++k) {
-    const uint32_t x = t[k] + Pv[k];
-    const uint32_t y = x + carry;
-    carry = (x < t[k]) | (y < x);
-    s[k] = y;
-  }
+  for (int k = 1; k < W - 1; ++k) asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s[k]) : "r"(t[k]), "r"(Pv[k]));
+  asm volatile("addc.u32 %0, %1, %2;" : "=r"(s[W - 1]) : "r"(t[W - 1]), "r"(Pv[W - 1]));
   uint32_t pin = hin > 0 ? 1u : 0u, min_ = hin < 0 ? 1u : 0u;
 #pragma unroll
   for (int k = 0; k < W; ++k) {
@@ -195,78 +240,91 @@ __device__ __forceinline__ int tb_column(const uint32_t* __restrict__ eq, uint32
   return (int)pin - (int)min_;
 }
 
+// First list place whose band offset is >= v.
+__device__ __forceinline__ uint32_t tb_lower(const unsigned long long* __restrict__ offs, uint32_t n,
+                                             unsigned long long v) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(offs + mid) < v) lo = mid + 1u;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ unsigned char* tb_slot(const TbArgs& a, uint32_t k) {
+  return a.scratch + ((__ldg(a.offs + k) - a.unit_lo) << kTbUnitShift);
+}
+
+// Shared memory per warp: 32 lanes x 5 bases x W words.
 template <int W>
-__device__ void tb_forward_one(const TbArgs& a, const TbGeom& g, uint32_t id, uint32_t* __restrict__ sm,
-                               uint4* __restrict__ slot) {
-  const int l = (int)(threadIdx.x & 31u);
-  const bool on = (uint32_t)l < g.L;
-  // the lane's W words of the top-aligned query, all five bases: sm[(l*5 + c)*W + k]
-  if (on) {
-    const int nw = (int)((g.m + 31u) >> 5);
-    const int pw = (int)(g.p >> 5), ps = (int)(g.p & 31u);
-    for (int c = 0; c < 5; ++c)
+__global__ void __launch_bounds__(128) k_tb_forward(TbArgs a) {
+  extern __shared__ __align__(16) uint32_t tb_smem[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t S = a.seg, G = 32u / S;
+  const uint32_t seg = lane / S, r = lane % S;
+  uint32_t* sm = tb_smem + (warp * 32u + lane) * 5u * W;  // this lane's [base][W]
+  const uint32_t klo = tb_lower(a.offs, a.count, a.unit_lo), khi = tb_lower(a.offs, a.count, a.unit_hi);
+  for (uint32_t base = klo + (blockIdx.x * 4u + warp) * G; base < khi; base += gridDim.x * 4u * G) {
+    const uint32_t k = base + seg;
+    TbGeom g;
+    uint32_t id = 0;
+    bool have = false;
+    if (k < khi) {
+      id = a.ids[k];
+      have = tb_setup(a, id, a.results[id], W, g) == 0u;
+    }
+    const bool on = have && r < g.L;
+    const uint32_t steps = __reduce_max_sync(FULL_MASK, have ? g.c1 + g.L - 1u : 0u);
+    uint4* slot = have ? reinterpret_cast<uint4*>(tb_slot(a, k)) : nullptr;
+    if (on) {
+      // the lane's W words of the top-aligned query, all five bases
+      const int nw = (int)((g.m + 31u) >> 5);
+      const int pw = (int)(g.p >> 5), ps = (int)(g.p & 31u);
+      for (int c = 0; c < 5; ++c)
 #pragma unroll
-      for (int k = 0; k < W; ++k) {
-        const int x = l * W + k - pw;
-        const uint32_t hi = qword(a.peq, g.pos_entry, nw, c, x);
-        const uint32_t lo = qword(a.peq, g.pos_entry, nw, c, x - 1);
-        sm[(l * 5 + c) * W + k] = ps ? __funnelshift_r(lo, hi, 32 - ps) : hi;
-      }
-  }
-  __syncwarp();
-  uint32_t Pv[W], Mv[W], ph[W], mh[W];
+        for (int kk = 0; kk < W; ++kk) {
+          const int x = (int)r * W + kk - pw;
+          const uint32_t hi = qword(a.peq, g.pos_entry, nw, c, x);
+          const uint32_t lo = qword(a.peq, g.pos_entry, nw, c, x - 1);
+          sm[c * W + kk] = ps ? __funnelshift_r(lo, hi, 32 - ps) : hi;
+        }
+    }
+    __syncwarp();
+    uint32_t Pv[W], Mv[W], ph[W], mh[W];
 #pragma unroll
-  for (int k = 0; k < W; ++k) {
-    Pv[k] = FULL_MASK;
-    Mv[k] = 0u;
-  }
-  int hout = 0;
-  uint32_t top = 32u * g.tw;  // D at the top row, column 0 (lane L-1)
-  const uint32_t steps = g.c1 + g.L - 1u;
-  for (uint32_t t = 0; t < steps; ++t) {
-    int hin = __shfl_up_sync(FULL_MASK, hout, 1);
-    if (l == 0) hin = 0;
-    const int j = (int)t - l;  // 0-based text base of this lane's column
-    hout = 0;
-    if (on && j >= 0 && (uint32_t)j < g.c1) {
-      const uint32_t code = ref_code(a.ref, g.start + (unsigned long long)j, a.ref_words);
-      hout = tb_column<W>(sm + (l * 5 + (int)code) * W, Pv, Mv, hin, ph, mh);
-      const uint32_t j1 = (uint32_t)j + 1u;
-      if (l == (int)g.L - 1) top += (uint32_t)hout;
-      if (j1 >= g.a0) {
-        const uint32_t xlo = tb_xlo(g, j1);
-        uint4* col = slot + (size_t)(j1 - g.a0) * g.B;
+    for (int kk = 0; kk < W; ++kk) {
+      Pv[kk] = FULL_MASK;
+      Mv[kk] = 0u;
+    }
+    int hout = 0;
+    uint32_t top = on ? 32u * g.tw : 0u;  // D at the top row, column 0 (last lane of the segment)
+    const uint32_t x0 = r * W;            // the lane's first word
+    for (uint32_t t = 0; t < steps; ++t) {
+      int hin = __shfl_up_sync(FULL_MASK, hout, 1, S);
+      if (r == 0) hin = 0;
+      const int j = (int)t - (int)r;  // 0-based text base of this lane's column
+      hout = 0;
+      if (on && j >= 0 && (uint32_t)j < g.c1) {
+        const uint32_t code = ref_code(a.ref, g.start + (unsigned long long)j, a.ref_words);
+        hout = tb_column<W>(sm + code * W, Pv, Mv, hin, ph, mh);
+        const uint32_t j1 = (uint32_t)j + 1u;
+        if (r == g.L - 1u) top += (uint32_t)hout;
+        if (j1 >= g.a0) {
+          const uint32_t xlo = tb_xlo(g, j1);
+          if (x0 < xlo + g.B && xlo < x0 + W) {  // the lane's words meet the band
+            uint4* col = slot + (size_t)(j1 - g.a0) * g.B;
 #pragma unroll
-        for (int k = 0; k < W; ++k) {
-          const uint32_t x = (uint32_t)(l * W + k);
-          if (x >= xlo && x < xlo + g.B) col[x - xlo] = make_uint4(Pv[k], Mv[k], ph[k], mh[k]);
+            for (int kk = 0; kk < W; ++kk) {
+              const uint32_t d = x0 + kk - xlo;  // wraps above B when below the band
+              if (d < g.B) col[d] = make_uint4(Pv[kk], Mv[kk], ph[kk], mh[kk]);
+            }
+          }
         }
       }
     }
-  }
-  // the recomputed score at the end column must be the result's
-  if (l == (int)g.L - 1 && top - g.p != g.s) a.alns[id].y = kTbInconsistent;
-}
-
-template <int WMAX>
-__global__ void __launch_bounds__(128) k_tb_forward(TbArgs a, uint32_t first, uint32_t cnt) {
-  extern __shared__ uint32_t tb_smem[];
-  const uint32_t warp = threadIdx.x >> 5;
-  uint32_t* sm = tb_smem + warp * (32u * 5u * WMAX);
-  for (uint32_t k = blockIdx.x * 4u + warp; k < cnt; k += gridDim.x * 4u) {
-    const uint32_t id = a.ids[first + k];
-    TbGeom g;
-    if (tb_setup(a, id, a.results[id], g) != 0u) continue;  // warp-uniform
-    uint4* slot = reinterpret_cast<uint4*>(a.scratch + (size_t)k * a.slot_bytes);
-    switch (g.wl) {
-      case 1: tb_forward_one<1>(a, g, id, sm, slot); break;
-      case 2: if (WMAX >= 2) tb_forward_one<(WMAX >= 2 ? 2 : 1)>(a, g, id, sm, slot); break;
-      case 4: if (WMAX >= 4) tb_forward_one<(WMAX >= 4 ? 4 : 1)>(a, g, id, sm, slot); break;
-      case 8: if (WMAX >= 8) tb_forward_one<(WMAX >= 8 ? 8 : 1)>(a, g, id, sm, slot); break;
-      case 16: if (WMAX >= 16) tb_forward_one<(WMAX >= 16 ? 16 : 1)>(a, g, id, sm, slot); break;
-      case 32: if (WMAX >= 32) tb_forward_one<(WMAX >= 32 ? 32 : 1)>(a, g, id, sm, slot); break;
-      default: break;
-    }
+    // the recomputed score at the end column must be the result's
+    if (on && r == g.L - 1u && top - g.p != g.s) a.alns[id].y = kTbInconsistent;
     __syncwarp();
   }
 }
@@ -275,18 +333,48 @@ __device__ __forceinline__ int tb_delta(uint32_t p, uint32_t m, uint32_t sh) {
   return (int)((p >> sh) & 1u) - (int)((m >> sh) & 1u);
 }
 
-__global__ void __launch_bounds__(128) k_tb_walk(TbArgs a, uint32_t first, uint32_t cnt) {
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
-    const uint32_t id = a.ids[first + k];
+// Word x of column j1's band, tagged with x; a zero word tagged 0xFFFFFFFF
+// when the column is not kept (outside [max(1, a0), c1]; a column index that
+// wrapped below zero lands above c1) or x lies outside its band.
+struct TbCol {
+  uint4 v;
+  uint32_t x;
+};
+
+__device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const TbGeom& g, uint32_t j1, uint32_t x) {
+  TbCol c;
+  c.v = make_uint4(0u, 0u, 0u, 0u);
+  c.x = 0xFFFFFFFFu;
+  if (j1 >= 1u && j1 >= g.a0 && j1 <= g.c1) {
+    const uint32_t xa = tb_xlo(g, j1);
+    if (x >= xa && x < xa + g.B) {
+      c.v = __ldcg(slot + (size_t)(j1 - g.a0) * g.B + (x - xa));
+      c.x = x;
+    }
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(128) k_tb_walk(TbArgs a) {
+  const uint32_t klo = tb_lower(a.offs, a.count, a.unit_lo), khi = tb_lower(a.offs, a.count, a.unit_hi);
+  for (uint32_t k = klo + blockIdx.x * blockDim.x + threadIdx.x; k < khi; k += gridDim.x * blockDim.x) {
+    const uint32_t id = a.ids[k];
     TbGeom g;
-    if (tb_setup(a, id, a.results[id], g) != 0u) continue;
+    if (tb_setup(a, id, a.results[id], a.wl, g) != 0u) continue;
     if (a.alns[id].y == kTbInconsistent) continue;
-    const uint4* slot = reinterpret_cast<const uint4*>(a.scratch + (size_t)k * a.slot_bytes);
+    const uint4* slot = reinterpret_cast<const uint4*>(tb_slot(a, k));
     uint32_t* out = a.ops + (size_t)id * a.max_ops;
     const int nw = (int)((g.m + 31u) >> 5);
     uint32_t i = g.m, j1 = g.c1;
     uint32_t nruns = 0, cur = 0, len = 0;
     bool bad = false;
+    // c0: column j1; c1..c4: columns j1-1 .. j1-4 (fetched ahead); all at word xw
+    uint32_t xw = 0xFFFFFFFFu;
+    TbCol c0, c1, c2, c3, c4;
+    // PEQ words of query word qw (five bases); text word twi
+    uint32_t qw = 0xFFFFFFFFu, q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
+    unsigned long long twi = ~0ull;
+    uint32_t twv = 0;
     // every step lowers i or j1: at most m + c1 steps
     while (i > 0u) {
       uint32_t op;
@@ -295,20 +383,46 @@ __global__ void __launch_bounds__(128) k_tb_walk(TbArgs a, uint32_t first, uint3
         --i;
       } else {
         const uint32_t bit = g.p + i - 1u, x = bit >> 5, sh = bit & 31u;
-        const uint32_t xa = tb_xlo(g, j1);
-        if (x < xa || x >= xa + g.B) { bad = true; break; }
-        const uint4 c = slot[(size_t)(j1 - g.a0) * g.B + (x - xa)];
-        const int h = tb_delta(c.z, c.w, sh), v = tb_delta(c.x, c.y, sh);
+        if (x != xw) {
+          xw = x;
+          c0 = tb_fetch(slot, g, j1, x);
+          c1 = tb_fetch(slot, g, j1 - 1u, x);
+          c2 = tb_fetch(slot, g, j1 - 2u, x);
+          c3 = tb_fetch(slot, g, j1 - 3u, x);
+          c4 = tb_fetch(slot, g, j1 - 4u, x);
+        }
+        if (c0.x != x) c0 = tb_fetch(slot, g, j1, x);
+        if (c0.x != x) {  // the path left the stored band: the data is inconsistent
+          bad = true;
+          break;
+        }
+        const uint32_t q = i - 1u;
+        if ((q >> 5) != qw) {
+          qw = q >> 5;
+          q0 = qword(a.peq, g.pos_entry, nw, 0, (int)qw);
+          q1 = qword(a.peq, g.pos_entry, nw, 1, (int)qw);
+          q2 = qword(a.peq, g.pos_entry, nw, 2, (int)qw);
+          q3 = qword(a.peq, g.pos_entry, nw, 3, (int)qw);
+          q4 = qword(a.peq, g.pos_entry, nw, 4, (int)qw);
+        }
+        const unsigned long long b = g.start + j1 - 1u;
+        if ((b >> 3) != twi) {
+          twi = b >> 3;
+          twv = sanitize_codes(ref_load(a.ref, (long long)twi, a.ref_words));
+        }
+        const uint32_t code = (twv >> (4u * (uint32_t)(b & 7u))) & 0xFu;
+        const uint32_t pq = code == 0 ? q0 : code == 1 ? q1 : code == 2 ? q2 : code == 3 ? q3 : q4;
+        const uint32_t match = (pq >> (q & 31u)) & 1u;
+        const int h = tb_delta(c0.v.z, c0.v.w, sh), v = tb_delta(c0.v.x, c0.v.y, sh);
         int vl = 1;  // column 0: D[i][0] = i
         if (j1 - 1u > 0u) {
-          const uint32_t xb = tb_xlo(g, j1 - 1u);
-          if (x < xb || x >= xb + g.B) { bad = true; break; }
-          const uint4 cl = slot[(size_t)(j1 - 1u - g.a0) * g.B + (x - xb)];
-          vl = tb_delta(cl.x, cl.y, sh);
+          if (c1.x != x) c1 = tb_fetch(slot, g, j1 - 1u, x);
+          if (c1.x != x) {
+            bad = true;
+            break;
+          }
+          vl = tb_delta(c1.v.x, c1.v.y, sh);
         }
-        const uint32_t code = ref_code(a.ref, g.start + j1 - 1u, a.ref_words);
-        const uint32_t q = i - 1u;
-        const uint32_t match = (qword(a.peq, g.pos_entry, nw, (int)code, (int)(q >> 5)) >> (q & 31u)) & 1u;
         if (h + vl == (int)(1u - match)) {
           op = match ? kOpEq : kOpX;
           --i;
@@ -319,6 +433,13 @@ __global__ void __launch_bounds__(128) k_tb_walk(TbArgs a, uint32_t first, uint3
         } else {
           op = kOpD;
           --j1;
+        }
+        if (op != kOpI) {  // one column to the left: shift the window, fetch one more
+          c0 = c1;
+          c1 = c2;
+          c2 = c3;
+          c3 = c4;
+          c4 = tb_fetch(slot, g, j1 >= 4u ? j1 - 4u : 0u, xw);
         }
       }
       if (len && op == cur) {
@@ -360,14 +481,32 @@ struct myersTraceback {
   uint64_t scratch_bytes;
   unsigned char* d_scratch;
   uint32_t* d_ids;
+  unsigned long long* d_offs;
   TbState* d_state;
   TbState* h_state;
+  cudaStream_t walk_stream;
+  cudaEvent_t fwd_done[2], walk_done[2];
   uint32_t last_count;
   uint32_t last_chunks;
 };
 
+static void tb_release(myersTraceback_t* t) {
+  cudaFree(t->d_scratch);
+  cudaFree(t->d_ids);
+  cudaFree(t->d_offs);
+  cudaFree(t->d_state);
+  cudaFreeHost(t->h_state);
+  for (int h = 0; h < 2; ++h) {
+    if (t->fwd_done[h]) cudaEventDestroy(t->fwd_done[h]);
+    if (t->walk_done[h]) cudaEventDestroy(t->walk_done[h]);
+  }
+  if (t->walk_stream) cudaStreamDestroy(t->walk_stream);
+  delete t;
+}
+
 extern "C" int myersTracebackCreate(myersTraceback_t** tb, uint64_t maxCandidates, uint64_t scratchBytes) {
-  if (tb == nullptr || maxCandidates == 0 || maxCandidates > 0xFFFFFFFFull || scratchBytes < (1u << 20))
+  if (tb == nullptr || maxCandidates == 0 || maxCandidates >= (1ull << (64 - kTbCountShift)) ||
+      scratchBytes < (1u << 20))
     return MYERS_E_INVALID_ARGUMENT;
   *tb = nullptr;
   myersTraceback_t* t = new myersTraceback_t();
@@ -375,16 +514,19 @@ extern "C" int myersTracebackCreate(myersTraceback_t** tb, uint64_t maxCandidate
   cudaError_t e = cudaGetDevice(&t->device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, t->device);
   t->capacity = maxCandidates;
-  t->scratch_bytes = scratchBytes;
-  if (e == cudaSuccess) e = cudaMalloc((void**)&t->d_scratch, scratchBytes);
+  t->scratch_bytes = scratchBytes & ~511ull;
+  if (e == cudaSuccess) e = cudaMalloc((void**)&t->d_scratch, t->scratch_bytes);
   if (e == cudaSuccess) e = cudaMalloc((void**)&t->d_ids, maxCandidates * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&t->d_offs, maxCandidates * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc((void**)&t->d_state, sizeof(TbState));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&t->h_state, sizeof(TbState), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&t->walk_stream, cudaStreamNonBlocking);
+  for (int h = 0; h < 2 && e == cudaSuccess; ++h) {
+    e = cudaEventCreateWithFlags(&t->fwd_done[h], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->walk_done[h], cudaEventDisableTiming);
+  }
   if (e != cudaSuccess) {
-    cudaFree(t->d_scratch);
-    cudaFree(t->d_ids);
-    cudaFree(t->d_state);
-    delete t;
+    tb_release(t);
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? MYERS_E_INSUFFICIENT_MEM_GPU : cuda_fail(e, "myersTracebackCreate");
   }
@@ -396,28 +538,26 @@ extern "C" int myersTracebackDestroy(myersTraceback_t* tb) {
   if (tb == nullptr) return MYERS_E_INVALID_ARGUMENT;
   cudaSetDevice(tb->device);
   cudaDeviceSynchronize();
-  cudaFree(tb->d_scratch);
-  cudaFree(tb->d_ids);
-  cudaFree(tb->d_state);
-  cudaFreeHost(tb->h_state);
-  delete tb;
+  tb_release(tb);
   return MYERS_SUCCESS;
 }
 
 extern "C" uint32_t myersTracebackLastCount(const myersTraceback_t* tb) { return tb ? tb->last_count : 0u; }
 extern "C" uint32_t myersTracebackLastChunks(const myersTraceback_t* tb) { return tb ? tb->last_chunks : 0u; }
 
-template <int WMAX>
-static cudaError_t launch_tb_forward(const TbArgs& a, uint32_t first, uint32_t cnt, int num_sms, cudaStream_t s) {
-  const size_t smem = 4u * 32u * 5u * WMAX * sizeof(uint32_t);
+template <int W>
+static cudaError_t launch_tb_forward(const TbArgs& a, uint32_t cnt, int num_sms, cudaStream_t s) {
+  // cnt: an upper estimate of the chunk's candidates (the kernel finds its range)
+  const size_t smem = 4u * 32u * 5u * W * sizeof(uint32_t);
   if (smem > 48u * 1024u) {  // per function and device; cheap to repeat
-    cudaError_t e = cudaFuncSetAttribute(k_tb_forward<WMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_tb_forward<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  uint32_t blocks = (cnt + 3u) / 4u;
+  const uint32_t per_block = 4u * (32u / a.seg);
+  uint32_t blocks = (cnt + per_block - 1u) / per_block;
   const uint32_t cap = (uint32_t)num_sms * 16u;
   if (blocks > cap) blocks = cap;
-  k_tb_forward<WMAX><<<blocks, 128, smem, s>>>(a, first, cnt);
+  k_tb_forward<W><<<blocks, 128, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -429,11 +569,9 @@ extern "C" int myersTraceback(myersTraceback_t* tb, const myersReference_t* ref,
   if (tb == nullptr || ref == nullptr || !(distance >= 0.0f) || !std::isfinite(distance) ||
       (windowMode != MYERS_WINDOW_ALIGNED && windowMode != MYERS_WINDOW_EXACT) || maxOpsPerCandidate == 0)
     return MYERS_E_INVALID_ARGUMENT;
-  if (numCandidates == 0) {
-    tb->last_count = 0;
-    tb->last_chunks = 0;
-    return MYERS_SUCCESS;
-  }
+  tb->last_count = 0;
+  tb->last_chunks = 0;
+  if (numCandidates == 0) return MYERS_SUCCESS;
   if (d_peq == nullptr || d_qinfo == nullptr || d_cands == nullptr || d_results == nullptr || d_ops == nullptr ||
       d_alignments == nullptr)
     return MYERS_E_INVALID_ARGUMENT;
@@ -460,42 +598,60 @@ extern "C" int myersTraceback(myersTraceback_t* tb, const myersReference_t* ref,
   a.ops = d_ops;
   a.max_ops = maxOpsPerCandidate;
   a.alns = reinterpret_cast<uint4*>(d_alignments);
-  a.ids = tb->d_ids;
   a.st = tb->d_state;
-  a.scratch = tb->d_scratch;
   if ((e = cudaMemsetAsync(tb->d_state, 0, sizeof(TbState), s)) != cudaSuccess) return cuda_fail(e, "memset");
   uint32_t blocks = (numCandidates + 255u) / 256u;
   if (blocks > (uint32_t)tb->num_sms * 8u) blocks = (uint32_t)tb->num_sms * 8u;
-  k_tb_select<<<blocks, 256, 0, s>>>(a);
+  k_tb_select<<<blocks, 256, 0, s>>>(a, tb->d_ids, tb->d_offs);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "k_tb_select");
   // the pass count depends on how many candidates are traced and their band sizes
   if ((e = cudaMemcpyAsync(tb->h_state, tb->d_state, sizeof(TbState), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return cuda_fail(e, "traceback count");
   const TbState st = *tb->h_state;
-  tb->last_count = st.count;
-  tb->last_chunks = 0;
-  if (st.count == 0) return MYERS_SUCCESS;
-  const unsigned long long slot = (st.max_slot + 255ull) & ~255ull;
-  const unsigned long long per = tb->scratch_bytes / slot;
-  if (per == 0) return MYERS_E_CAPACITY;  // one candidate's band does not fit the scratch
-  a.slot_bytes = slot;
-  for (uint32_t first = 0; first < st.count; first += (uint32_t)per) {
-    const uint32_t cnt = (uint32_t)(st.count - first < per ? st.count - first : per);
-    switch (st.max_wl) {
-      case 1: e = launch_tb_forward<1>(a, first, cnt, tb->num_sms, s); break;
-      case 2: e = launch_tb_forward<2>(a, first, cnt, tb->num_sms, s); break;
-      case 4: e = launch_tb_forward<4>(a, first, cnt, tb->num_sms, s); break;
-      case 8: e = launch_tb_forward<8>(a, first, cnt, tb->num_sms, s); break;
-      case 16: e = launch_tb_forward<16>(a, first, cnt, tb->num_sms, s); break;
-      default: e = launch_tb_forward<32>(a, first, cnt, tb->num_sms, s); break;
+  const uint32_t count = (uint32_t)(st.packed >> kTbCountShift);
+  const unsigned long long total = st.packed & kTbUnitMask;
+  tb->last_count = count;
+  if (count == 0) return MYERS_SUCCESS;
+  a.wl = tb_words_per_lane(st.max_words);
+  const uint32_t lanes = (st.max_words + a.wl - 1u) / a.wl;
+  a.seg = 1;
+  while (a.seg < lanes) a.seg <<= 1;
+  a.ids = tb->d_ids;
+  a.offs = tb->d_offs;
+  a.count = count;
+  // a chunk holds the candidates whose offsets start in a window of H units;
+  // the last of them ends within H + max_units <= half the scratch
+  const unsigned long long half_units = (tb->scratch_bytes / 2) >> kTbUnitShift;
+  if (half_units <= st.max_units) return MYERS_E_CAPACITY;  // one band does not fit half the scratch
+  const unsigned long long H = half_units - st.max_units;
+  const unsigned long long chunks = (total + H - 1ull) / H;
+  const uint32_t est = (uint32_t)((unsigned long long)count * (H < total ? H : total) / total) + 1u;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const int h = (int)(c & 1u);
+    TbArgs ca = a;
+    ca.unit_lo = c * H;
+    ca.unit_hi = ca.unit_lo + H;
+    ca.scratch = tb->d_scratch + (size_t)h * (half_units << kTbUnitShift);
+    if (c >= 2 && (e = cudaStreamWaitEvent(s, tb->walk_done[h], 0)) != cudaSuccess) return cuda_fail(e, "wait");
+    switch (a.wl) {
+      case 8: e = launch_tb_forward<8>(ca, est, tb->num_sms, s); break;
+      case 16: e = launch_tb_forward<16>(ca, est, tb->num_sms, s); break;
+      default: e = launch_tb_forward<32>(ca, est, tb->num_sms, s); break;
     }
     if (e != cudaSuccess) return cuda_fail(e, "k_tb_forward");
-    uint32_t wb = (cnt + 127u) / 128u;
+    if ((e = cudaEventRecord(tb->fwd_done[h], s)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(tb->walk_stream, tb->fwd_done[h], 0)) != cudaSuccess)
+      return cuda_fail(e, "event");
+    uint32_t wb = (est + 127u) / 128u;
     if (wb > (uint32_t)tb->num_sms * 16u) wb = (uint32_t)tb->num_sms * 16u;
-    k_tb_walk<<<wb, 128, 0, s>>>(a, first, cnt);
+    k_tb_walk<<<wb, 128, 0, tb->walk_stream>>>(ca);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "k_tb_walk");
-    ++tb->last_chunks;
+    if ((e = cudaEventRecord(tb->walk_done[h], tb->walk_stream)) != cudaSuccess) return cuda_fail(e, "event");
   }
+  const uint32_t c = (uint32_t)chunks;
+  tb->last_chunks = c;
+  // the caller's stream resumes after the last walk
+  if ((e = cudaStreamWaitEvent(s, tb->walk_done[(c - 1u) & 1u], 0)) != cudaSuccess) return cuda_fail(e, "wait");
   return MYERS_SUCCESS;
 }

@@ -65,7 +65,7 @@ def test_traceback_long_reads(mg, orc, tbdata):
 
 def test_traceback_small_scratch_and_ops(mg, orc, tbdata):
     w = tbdata["ws"][5]
-    aln, chunks = _check(mg, orc, tbdata, w, 10 ** 6, 1024, scratch=1 << 20)
+    aln, chunks = _check(mg, orc, tbdata, w, 10 ** 6, 1024, scratch=4 << 20)
     assert chunks > 1
     # room for 3 runs only: the count is reported, the record otherwise the same
     aln, _ = _check(mg, orc, tbdata, w, 10 ** 6, 3)
