@@ -425,7 +425,9 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
   }
   if (path == MYERS_PATH_PLAIN && plan.num_cfg == 1) {
     const Shape sh = plan.shape[0];
-    CU(launch_plain(sh.variant, sh.L, in, nullptr, nullptr, 0, 0, in.num_cands, s, ctx->num_sms));
+    uint32_t* next = &ctx->d_state->next[0];  // the launch's tile counter
+    CU(cudaMemsetAsync(next, 0, sizeof(uint32_t), s));
+    CU(launch_plain(sh.variant, sh.L, in, nullptr, nullptr, 0, 0, in.num_cands, next, s, ctx->num_sms));
     ctx->last_launches = 1;
     return MYERS_SUCCESS;
   }
@@ -440,8 +442,8 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     first_plain = plan.num_batched;
   }
   for (uint32_t c = first_plain; c < plan.num_cfg; ++c) {
-    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, ctx->d_ids, ctx->d_state, (int)c, 0, 0, s,
-                    ctx->num_sms));
+    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, ctx->d_ids, ctx->d_state, (int)c, 0, 0,
+                    &ctx->d_state->next[c], s, ctx->num_sms));
     ++launches;
   }
   ctx->last_launches = launches;
@@ -1001,6 +1003,7 @@ extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refW
   if (plan.num_batched > 0)
     CU(launch_batched(in, d_ids, plan, d_state, s, dev.num_sms, batched_tile_bound(plan, numCandidates)));
   for (uint32_t c = plan.num_batched; c < plan.num_cfg; ++c)
-    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, d_ids, d_state, (int)c, 0, 0, s, dev.num_sms));
+    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, d_ids, d_state, (int)c, 0, 0, &d_state->next[c], s,
+                    dev.num_sms));
   return MYERS_SUCCESS;
 }

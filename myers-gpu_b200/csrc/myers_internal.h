@@ -73,6 +73,7 @@ struct BucketState {
   uint32_t total_tiles;          // tiles of the first num_batched shapes
   uint32_t queue;                // persistent kernel work counter
   uint32_t pad[2];
+  uint32_t next[kMaxCfg];        // plain launches: next warp tile per shape
 };
 
 struct DevInputs {
@@ -116,9 +117,10 @@ int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_
 
 // One plain launch of variant v. With d_state == nullptr the candidates are
 // indices [first, first+count) (no bucketing); otherwise shape `cfg`'s range
-// of the sorted id array, read from d_state on the device.
+// of the sorted id array, read from d_state on the device. d_next: the
+// launch's warp-tile counter, zero when the launch starts.
 cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
-                         int cfg, uint32_t first, uint32_t count, cudaStream_t s, int num_sms);
+                         int cfg, uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms);
 
 // The persistent batched launch over the plan's first num_batched shapes;
 // the grid is the device's resident capacity or, for small batches, one

@@ -421,12 +421,13 @@ __host__ __device__ constexpr uint32_t warp_words() {
   return (uint32_t)Layout<W, MULTI>::WORDS;
 }
 
-// Plain launch: one shape over a contiguous range of (sorted) candidates,
-// grid-stride over warp tiles.
+// Plain launch: one shape over a contiguous range of (sorted) candidates.
+// Warps take warp tiles from a device counter (`next`, zero at launch), so
+// SMs that run ahead take more tiles and the launch ends evenly.
 template <int W, bool MULTI>
 __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __restrict__ ids,
                                                const BucketState* __restrict__ st, int cfg, uint32_t first,
-                                               uint32_t count, int L) {
+                                               uint32_t count, int L, uint32_t* __restrict__ next) {
   extern __shared__ __align__(16) uint32_t smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   if (st != nullptr) {
@@ -436,8 +437,11 @@ __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __r
   const int nseg = MULTI ? 32 / L : 32;
   uint32_t* wsmem = smem + wib * warp_words<W, MULTI>();
   const uint32_t tiles = (count + nseg - 1) / nseg;
-  const uint32_t wpb = blockDim.x >> 5;
-  for (uint32_t t = blockIdx.x * wpb + wib; t < tiles; t += gridDim.x * wpb) {
+  while (true) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(next, 1u);
+    t = __shfl_sync(FULL_MASK, t, 0);
+    if (t >= tiles) break;
     const uint32_t f = t * nseg;
     const uint32_t cnt = min((uint32_t)nseg, count - f);
     process_tile<W, MULTI>(in, ids, first + f, cnt, L, wsmem, lane);
@@ -619,7 +623,7 @@ __global__ void k_lop3_probe(uint32_t* out, int iters) {
 
 // ---- host-side launchers ----
 
-using PlainFn = void (*)(DevInputs, const uint32_t*, const BucketState*, int, uint32_t, uint32_t, int);
+using PlainFn = void (*)(DevInputs, const uint32_t*, const BucketState*, int, uint32_t, uint32_t, int, uint32_t*);
 
 template <int V>
 constexpr PlainFn plain_fn() {
@@ -649,7 +653,7 @@ static int blocks_per_sm(const void* fn, int threads, size_t smem) {
 }
 
 cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
-                         int cfg, uint32_t first, uint32_t count, cudaStream_t s, int num_sms) {
+                         int cfg, uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms) {
   const PlainFn fn = kPlainTable.f[v];
   const int threads = 128;
   const int Lr = variant_multi(v) ? L : 1;
@@ -665,7 +669,7 @@ cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_id
     if (need < grid) grid = need;
     if (grid == 0) return cudaSuccess;
   }
-  fn<<<grid, threads, smem, s>>>(in, d_ids, d_state, cfg, first, count, Lr);
+  fn<<<grid, threads, smem, s>>>(in, d_ids, d_state, cfg, first, count, Lr, d_next);
   return cudaGetLastError();
 }
 
