@@ -56,6 +56,8 @@ struct TbState {
   unsigned long long packed;
   unsigned int max_words;  // longest query among them (32-bit words)
   unsigned int max_units;  // largest band store (256-byte units), for any words per lane
+  unsigned int max_inv_words;  // ~(shortest query's words): zero-initialised like the rest
+  unsigned int next[2][2];  // per scratch half: work counters of the forward pass and the walk
 };
 
 struct TbArgs {
@@ -79,6 +81,8 @@ struct TbArgs {
   TbState* st;
   unsigned char* scratch;          // this chunk's half
   unsigned long long unit_lo, unit_hi;  // this chunk: offsets in [unit_lo, unit_hi)
+  unsigned int* next;              // this chunk's counters: [0] forward groups, [1] walk candidates
+  int fwd_counter;                 // the forward pass takes groups from next[0] (else a static share)
   uint32_t wl;   // words per lane of this call
   uint32_t seg;  // lanes per candidate segment (power of two)
 };
@@ -170,6 +174,7 @@ __global__ void k_tb_select(TbArgs a, uint32_t* ids, unsigned long long* offs) {
         rec.y = 0u;
         units = (uint32_t)((tb_slot_bound(g) + (1ull << kTbUnitShift) - 1ull) >> kTbUnitShift);
         atomicMax(&a.st->max_words, (g.m + 31u) >> 5);
+        atomicMax(&a.st->max_inv_words, ~((g.m + 31u) >> 5));
         atomicMax(&a.st->max_units, units);
       }
       a.alns[id] = rec;
@@ -265,7 +270,21 @@ __global__ void __launch_bounds__(128) k_tb_forward(TbArgs a) {
   const uint32_t seg = lane / S, r = lane % S;
   uint32_t* sm = tb_smem + (warp * 32u + lane) * 5u * W;  // this lane's [base][W]
   const uint32_t klo = tb_lower(a.offs, a.count, a.unit_lo), khi = tb_lower(a.offs, a.count, a.unit_hi);
-  for (uint32_t base = klo + (blockIdx.x * 4u + warp) * G; base < khi; base += gridDim.x * 4u * G) {
+  // Groups of G candidates: with fwd_counter, warps take them from the
+  // chunk's counter (queries of mixed lengths: uneven groups); else warp w
+  // takes groups w, w + warps, ... (one query length: even groups, and blocks
+  // that exit early leave room for the previous chunk's walk).
+  const uint32_t nwarps = gridDim.x * 4u;
+  uint32_t gi = blockIdx.x * 4u + warp;
+  while (true) {
+    if (a.fwd_counter) {
+      uint32_t v = 0;
+      if (lane == 0) v = atomicAdd(&a.next[0], 1u);
+      gi = __shfl_sync(FULL_MASK, v, 0);
+    }
+    const uint32_t base = klo + gi * G;
+    if (base >= khi) break;
+    if (!a.fwd_counter) gi += nwarps;
     const uint32_t k = base + seg;
     TbGeom g;
     uint32_t id = 0;
@@ -355,118 +374,130 @@ __device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const 
   return c;
 }
 
-__global__ void __launch_bounds__(128) k_tb_walk(TbArgs a) {
-  const uint32_t klo = tb_lower(a.offs, a.count, a.unit_lo), khi = tb_lower(a.offs, a.count, a.unit_hi);
-  for (uint32_t k = klo + blockIdx.x * blockDim.x + threadIdx.x; k < khi; k += gridDim.x * blockDim.x) {
-    const uint32_t id = a.ids[k];
-    TbGeom g;
-    if (tb_setup(a, id, a.results[id], a.wl, g) != 0u) continue;
-    if (a.alns[id].y == kTbInconsistent) continue;
-    const uint4* slot = reinterpret_cast<const uint4*>(tb_slot(a, k));
-    uint32_t* out = a.ops + (size_t)id * a.max_ops;
-    const int nw = (int)((g.m + 31u) >> 5);
-    uint32_t i = g.m, j1 = g.c1;
-    uint32_t nruns = 0, cur = 0, len = 0;
-    bool bad = false;
-    // c0: column j1; c1..c4: columns j1-1 .. j1-4 (fetched ahead); all at word xw
-    uint32_t xw = 0xFFFFFFFFu;
-    TbCol c0, c1, c2, c3, c4;
-    // PEQ words of query word qw (five bases); text word twi
-    uint32_t qw = 0xFFFFFFFFu, q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
-    unsigned long long twi = ~0ull;
-    uint32_t twv = 0;
-    // every step lowers i or j1: at most m + c1 steps
-    while (i > 0u) {
-      uint32_t op;
-      if (j1 <= g.a0) {
-        op = kOpI;  // only the query base alone is left (column 0, or the first kept column)
-        --i;
-      } else {
-        const uint32_t bit = g.p + i - 1u, x = bit >> 5, sh = bit & 31u;
-        if (x != xw) {
-          xw = x;
-          c0 = tb_fetch(slot, g, j1, x);
-          c1 = tb_fetch(slot, g, j1 - 1u, x);
-          c2 = tb_fetch(slot, g, j1 - 2u, x);
-          c3 = tb_fetch(slot, g, j1 - 3u, x);
-          c4 = tb_fetch(slot, g, j1 - 4u, x);
-        }
-        if (c0.x != x) c0 = tb_fetch(slot, g, j1, x);
-        if (c0.x != x) {  // the path left the stored band: the data is inconsistent
+// The walk of list place k (a traced candidate of this chunk).
+__device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
+  const uint32_t id = a.ids[k];
+  TbGeom g;
+  if (tb_setup(a, id, a.results[id], a.wl, g) != 0u) return;
+  if (a.alns[id].y == kTbInconsistent) return;
+  const uint4* slot = reinterpret_cast<const uint4*>(tb_slot(a, k));
+  uint32_t* out = a.ops + (size_t)id * a.max_ops;
+  const int nw = (int)((g.m + 31u) >> 5);
+  uint32_t i = g.m, j1 = g.c1;
+  uint32_t nruns = 0, cur = 0, len = 0;
+  bool bad = false;
+  // c0: column j1; c1..c4: columns j1-1 .. j1-4 (fetched ahead); all at word xw
+  uint32_t xw = 0xFFFFFFFFu;
+  TbCol c0, c1, c2, c3, c4;
+  // PEQ words of query word qw (five bases); text word twi
+  uint32_t qw = 0xFFFFFFFFu, q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
+  unsigned long long twi = ~0ull;
+  uint32_t twv = 0;
+  // every step lowers i or j1: at most m + c1 steps
+  while (i > 0u) {
+    uint32_t op;
+    if (j1 <= g.a0) {
+      op = kOpI;  // only the query base alone is left (column 0, or the first kept column)
+      --i;
+    } else {
+      const uint32_t bit = g.p + i - 1u, x = bit >> 5, sh = bit & 31u;
+      if (x != xw) {
+        xw = x;
+        c0 = tb_fetch(slot, g, j1, x);
+        c1 = tb_fetch(slot, g, j1 - 1u, x);
+        c2 = tb_fetch(slot, g, j1 - 2u, x);
+        c3 = tb_fetch(slot, g, j1 - 3u, x);
+        c4 = tb_fetch(slot, g, j1 - 4u, x);
+      }
+      if (c0.x != x) c0 = tb_fetch(slot, g, j1, x);
+      if (c0.x != x) {  // the path left the stored band: the data is inconsistent
+        bad = true;
+        break;
+      }
+      const uint32_t q = i - 1u;
+      if ((q >> 5) != qw) {
+        qw = q >> 5;
+        q0 = qword(a.peq, g.pos_entry, nw, 0, (int)qw);
+        q1 = qword(a.peq, g.pos_entry, nw, 1, (int)qw);
+        q2 = qword(a.peq, g.pos_entry, nw, 2, (int)qw);
+        q3 = qword(a.peq, g.pos_entry, nw, 3, (int)qw);
+        q4 = qword(a.peq, g.pos_entry, nw, 4, (int)qw);
+      }
+      const unsigned long long b = g.start + j1 - 1u;
+      if ((b >> 3) != twi) {
+        twi = b >> 3;
+        twv = sanitize_codes(ref_load(a.ref, (long long)twi, a.ref_words));
+      }
+      const uint32_t code = (twv >> (4u * (uint32_t)(b & 7u))) & 0xFu;
+      const uint32_t pq = code == 0 ? q0 : code == 1 ? q1 : code == 2 ? q2 : code == 3 ? q3 : q4;
+      const uint32_t match = (pq >> (q & 31u)) & 1u;
+      const int h = tb_delta(c0.v.z, c0.v.w, sh), v = tb_delta(c0.v.x, c0.v.y, sh);
+      int vl = 1;  // column 0: D[i][0] = i
+      if (j1 - 1u > 0u) {
+        if (c1.x != x) c1 = tb_fetch(slot, g, j1 - 1u, x);
+        if (c1.x != x) {
           bad = true;
           break;
         }
-        const uint32_t q = i - 1u;
-        if ((q >> 5) != qw) {
-          qw = q >> 5;
-          q0 = qword(a.peq, g.pos_entry, nw, 0, (int)qw);
-          q1 = qword(a.peq, g.pos_entry, nw, 1, (int)qw);
-          q2 = qword(a.peq, g.pos_entry, nw, 2, (int)qw);
-          q3 = qword(a.peq, g.pos_entry, nw, 3, (int)qw);
-          q4 = qword(a.peq, g.pos_entry, nw, 4, (int)qw);
-        }
-        const unsigned long long b = g.start + j1 - 1u;
-        if ((b >> 3) != twi) {
-          twi = b >> 3;
-          twv = sanitize_codes(ref_load(a.ref, (long long)twi, a.ref_words));
-        }
-        const uint32_t code = (twv >> (4u * (uint32_t)(b & 7u))) & 0xFu;
-        const uint32_t pq = code == 0 ? q0 : code == 1 ? q1 : code == 2 ? q2 : code == 3 ? q3 : q4;
-        const uint32_t match = (pq >> (q & 31u)) & 1u;
-        const int h = tb_delta(c0.v.z, c0.v.w, sh), v = tb_delta(c0.v.x, c0.v.y, sh);
-        int vl = 1;  // column 0: D[i][0] = i
-        if (j1 - 1u > 0u) {
-          if (c1.x != x) c1 = tb_fetch(slot, g, j1 - 1u, x);
-          if (c1.x != x) {
-            bad = true;
-            break;
-          }
-          vl = tb_delta(c1.v.x, c1.v.y, sh);
-        }
-        if (h + vl == (int)(1u - match)) {
-          op = match ? kOpEq : kOpX;
-          --i;
-          --j1;
-        } else if (v == 1) {
-          op = kOpI;
-          --i;
-        } else {
-          op = kOpD;
-          --j1;
-        }
-        if (op != kOpI) {  // one column to the left: shift the window, fetch one more
-          c0 = c1;
-          c1 = c2;
-          c2 = c3;
-          c3 = c4;
-          c4 = tb_fetch(slot, g, j1 >= 4u ? j1 - 4u : 0u, xw);
-        }
+        vl = tb_delta(c1.v.x, c1.v.y, sh);
       }
-      if (len && op == cur) {
-        ++len;
+      if (h + vl == (int)(1u - match)) {
+        op = match ? kOpEq : kOpX;
+        --i;
+        --j1;
+      } else if (v == 1) {
+        op = kOpI;
+        --i;
       } else {
-        if (len) {
-          if (nruns < a.max_ops) out[a.max_ops - 1u - nruns] = (len << 4) | cur;
-          ++nruns;
-        }
-        cur = op;
-        len = 1;
+        op = kOpD;
+        --j1;
+      }
+      if (op != kOpI) {  // one column to the left: shift the window, fetch one more
+        c0 = c1;
+        c1 = c2;
+        c2 = c3;
+        c3 = c4;
+        c4 = tb_fetch(slot, g, j1 >= 4u ? j1 - 4u : 0u, xw);
       }
     }
-    if (bad) {
-      a.alns[id].y = kTbInconsistent;
-      continue;
+    if (len && op == cur) {
+      ++len;
+    } else {
+      if (len) {
+        if (nruns < a.max_ops) out[a.max_ops - 1u - nruns] = (len << 4) | cur;
+        ++nruns;
+      }
+      cur = op;
+      len = 1;
     }
-    if (len) {
-      if (nruns < a.max_ops) out[a.max_ops - 1u - nruns] = (len << 4) | cur;
-      ++nruns;
-    }
-    // runs were written last first at the end of the region: move them to the front
-    if (nruns <= a.max_ops) {
-      const uint32_t src = a.max_ops - nruns;
-      for (uint32_t r = 0; r < nruns; ++r) out[r] = out[src + r];
-    }
-    a.alns[id] = make_uint4(j1, nruns, g.s, g.c1 - 1u);
+  }
+  if (bad) {
+    a.alns[id].y = kTbInconsistent;
+    return;
+  }
+  if (len) {
+    if (nruns < a.max_ops) out[a.max_ops - 1u - nruns] = (len << 4) | cur;
+    ++nruns;
+  }
+  // runs were written last first at the end of the region: move them to the front
+  if (nruns <= a.max_ops) {
+    const uint32_t src = a.max_ops - nruns;
+    for (uint32_t r = 0; r < nruns; ++r) out[r] = out[src + r];
+  }
+  a.alns[id] = make_uint4(j1, nruns, g.s, g.c1 - 1u);
+}
+
+__global__ void __launch_bounds__(128) k_tb_walk(TbArgs a) {
+  const uint32_t klo = tb_lower(a.offs, a.count, a.unit_lo), khi = tb_lower(a.offs, a.count, a.unit_hi);
+  const uint32_t lane = threadIdx.x & 31u;
+  while (true) {
+    // warps take 32 candidates at a time from the chunk's counter
+    uint32_t w0 = 0;
+    if (lane == 0) w0 = atomicAdd(&a.next[1], 32u);
+    const uint32_t base = klo + __shfl_sync(FULL_MASK, w0, 0);
+    if (base >= khi) break;
+    if (base + lane < khi) tb_walk_one(a, base + lane);
+    __syncwarp();
   }
 }
 
@@ -614,6 +645,7 @@ extern "C" int myersTraceback(myersTraceback_t* tb, const myersReference_t* ref,
   tb->last_count = count;
   if (count == 0) return MYERS_SUCCESS;
   a.wl = tb_words_per_lane(st.max_words);
+  a.fwd_counter = (~st.max_inv_words) != st.max_words;  // more than one query length
   const uint32_t lanes = (st.max_words + a.wl - 1u) / a.wl;
   a.seg = 1;
   while (a.seg < lanes) a.seg <<= 1;
@@ -633,7 +665,10 @@ extern "C" int myersTraceback(myersTraceback_t* tb, const myersReference_t* ref,
     ca.unit_lo = c * H;
     ca.unit_hi = ca.unit_lo + H;
     ca.scratch = tb->d_scratch + (size_t)h * (half_units << kTbUnitShift);
+    ca.next = tb->d_state->next[h];
     if (c >= 2 && (e = cudaStreamWaitEvent(s, tb->walk_done[h], 0)) != cudaSuccess) return cuda_fail(e, "wait");
+    // the half's walk of two chunks ago has finished: its counters may start again
+    if ((e = cudaMemsetAsync(ca.next, 0, 2 * sizeof(unsigned int), s)) != cudaSuccess) return cuda_fail(e, "memset");
     switch (a.wl) {
       case 8: e = launch_tb_forward<8>(ca, est, tb->num_sms, s); break;
       case 16: e = launch_tb_forward<16>(ca, est, tb->num_sms, s); break;
