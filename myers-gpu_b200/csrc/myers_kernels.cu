@@ -159,18 +159,24 @@ __device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t
   }
 }
 
-// (cur << 1) | (prev >> 31): the one-bit shift of a multi-word vector.
-// Mode 0 (default): one funnel shift on the ALU pipe. Mode 2: multiply-high
-// and multiply-add by an opaque two, on the FMA pipe -- fewer ALU
-// instructions but more instructions and latency in all; it loses at the
-// occupancy the single-lane shapes reach (measured).
-__device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k) {
-#if MYERS_SHIFT_MODE == 2
-  return cur * k.two + __umulhi(prev, k.two);
-#else
-  (void)k;
-  return __funnelshift_l(prev, cur, 1);
+#ifndef MYERS_FMA_SHIFT_MAX_W
+#define MYERS_FMA_SHIFT_MAX_W 8  // plain-100b +1.7% (measured); no change on wider shapes
 #endif
+
+// (cur << 1) | (prev >> 31): the one-bit shift of a multi-word vector.
+// On the ALU pipe: one funnel shift. On the FMA pipe: multiply-high and
+// multiply-add by an opaque two -- fewer ALU instructions but more
+// instructions and latency in all, which only pays where many warps are
+// resident (narrow shapes). FMA for shapes of at most MYERS_FMA_SHIFT_MAX_W
+// words (MYERS_SHIFT_MODE=2: all shapes).
+template <int W>
+__device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k) {
+  if constexpr (MYERS_SHIFT_MODE == 2 || W <= MYERS_FMA_SHIFT_MAX_W) {
+    return cur * k.two + __umulhi(prev, k.two);
+  } else {
+    (void)k;
+    return __funnelshift_l(prev, cur, 1);
+  }
 }
 
 // One text column over W words. With HIN, bit 31 of inP / inM is the
@@ -196,8 +202,8 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
     const uint32_t xh = (s[j] ^ pv) | e;
     const uint32_t ph = mv | ~(xh | pv);
     const uint32_t mh = pv & xh;
-    const uint32_t phs = shl1(php, ph, k);
-    const uint32_t mhs = shl1(mhp, mh, k);
+    const uint32_t phs = shl1<W>(php, ph, k);
+    const uint32_t mhs = shl1<W>(mhp, mh, k);
     Pv[j] = mhs | ~(xv | phs);
     Mv[j] = phs & xv;
     php = ph;
