@@ -5,7 +5,8 @@ shapes are every compiled variant that holds w words: one candidate per lane
 with W = w words (w <= 32), and a candidate spread over L = ceil(w/W) lanes
 for each multi-lane width W (the persistent kernel carries W <= 16). For every
 bucket 1..32 and a sample of longer ones, each shape is timed on a seeded
-workload of reads of 32*w bases (CUDA events, best of three after a warm-up);
+workload of reads of 32*w bases, about 1e13 cells (20K..4M candidates) so
+that every shape runs many waves (CUDA events, best of three after a warm-up);
 the fastest wins. Unsampled long buckets take the width of the nearest
 sampled bucket above them, with L = ceil(w/W).
 
@@ -68,7 +69,10 @@ def main():
     for w in buckets:
         m = 32 * w
         cells = 1.4 * m * m
-        n_cands = int(min(2_000_000, max(3000, 1e11 / cells)))
+        # large batches (about 1e13 cells: many waves of the widest shapes), so
+        # the choice is the shape that sustains the highest throughput rather
+        # than the one that best fills a GPU too large for the batch
+        n_cands = int(min(4_000_000, max(20_000, 1e13 / cells)))
         s = mg.spec(ref_size, max(1, n_cands // 11), 1000 + w, lengths=m, cands=11)
         wl = mg.make_workload(s, ref_words)
         n = len(wl["cands"])
@@ -128,7 +132,7 @@ def main():
     props = torch.cuda.get_device_properties(0)
     out = {"device": props.name, "sms": props.multi_processor_count, "distance": DIST,
            "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
-           "method": "per bucket: every compiled shape timed on reads of 32*w bases, best of 3 after a warm-up",
+           "method": "per bucket: every compiled shape timed on reads of 32*w bases (about 1e13 cells, 20K..4M candidates), best of 3 after a warm-up",
            "format": "plain/batched: words -> [W words per lane, L lanes per candidate]",
            "plain": {str(k): v for k, v in table["plain"].items()},
            "batched": {str(k): v for k, v in table["batched"].items()},
