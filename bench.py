@@ -174,7 +174,7 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
         pg = dist
     return world, rank, local, pg
@@ -189,6 +189,13 @@ def reduce_over_ranks(dist, elapsed_s, n_cands, cells, device):
     tot = torch.tensor([float(n_cands), float(cells)], dtype=torch.float64, device=device)
     dist.all_reduce(tot)
     return float(t.item()), float(tot[0].item()), float(tot[1].item())
+
+
+def all_ranks_true(dist, flag):
+    import torch
+    t = torch.tensor([1 if flag else 0], dtype=torch.int32, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    return bool(t.item())
 
 
 def make_inputs(mg, k, scale, seed_offset, num_reads=None):
@@ -369,9 +376,26 @@ def run_ours(args):
     # end to end through the drop-in API
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(mg, args, ref_words, ref_size, w, path)
+        e2e = run_e2e(mg, args, ref_words, ref_size, w, path, dist)
         if "_results" in e2e:
             e2e["results_equal_device"] = bool(np.array_equal(e2e.pop("_results"), res))
+        if dist is not None:
+            # whole job: all ranks' candidates over the slowest rank's seconds
+            # (every rank takes part in the same reductions, even without a value)
+            ok = bool(e2e.get("value"))
+            el_e2e = n_cands * args.steps / e2e["value"] if ok else float("inf")
+            el_max, all_c, _ = reduce_over_ranks(dist, el_e2e, n_cands, 0.0, "cuda")
+            ok = all_ranks_true(dist, ok)
+            same = all_ranks_true(dist, e2e.get("results_equal_device", False))
+            if ok:
+                e2e["value"] = all_c * args.steps / el_max
+                e2e["h2d_bytes_per_step"] *= world
+                e2e["d2h_bytes_per_step"] *= world
+                e2e["results_equal_device"] = same
+            else:
+                e2e = {"value": None, "unit": "candidates/s", "note": "a rank's buffers were too small"}
+    if dist is not None:
+        parity = all_ranks_true(dist, parity)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -404,7 +428,7 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(mg, args, ref_words, ref_size, w, path):
+def run_e2e(mg, args, ref_words, ref_size, w, path, dist=None):
     """The metric through the drop-in API from pinned host buffers: every
     step copies its inputs in and its results out. When the resident
     reference is much larger than L2 (3.1 Gbase: 1.55 GB), steps stream
@@ -456,6 +480,8 @@ def run_e2e(mg, args, ref_words, ref_size, w, path):
             del flush
         else:
             torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()  # ranks start the timed region together
             t = time.perf_counter()
             for i in range(min(nb, args.steps)):
                 send(i % nb)
