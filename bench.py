@@ -191,9 +191,10 @@ def reduce_over_ranks(dist, elapsed_s, n_cands, cells, device):
     return float(t.item()), float(tot[0].item()), float(tot[1].item())
 
 
-def all_ranks_true(dist, flag):
+def all_ranks_true(dist, flag, device="cuda"):
+    """True on every rank iff `flag` is true on every rank."""
     import torch
-    t = torch.tensor([1 if flag else 0], dtype=torch.int32, device="cuda")
+    t = torch.tensor([1 if flag else 0], dtype=torch.int32, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MIN)
     return bool(t.item())
 

@@ -1,5 +1,7 @@
 """The replicas path of bench.py on CPU: two gloo ranks, each with its own
-seeded batch, reduce to the slowest rank's time and the total work."""
+seeded batch, reduce to the slowest rank's time and the total work, and a
+flag (parity, results equal) holds for the job only if it holds on every
+rank."""
 import os
 import socket
 
@@ -25,7 +27,8 @@ def _rank_main(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     # each replica's own numbers: different times and batch sizes
     res = bench.reduce_over_ranks(dist, 1.0 + rank, 1000 * (rank + 1), 5e6 * (rank + 1), "cpu")
-    out.put((rank, res))
+    flags = (bench.all_ranks_true(dist, True, "cpu"), bench.all_ranks_true(dist, rank == 0, "cpu"))
+    out.put((rank, res + flags))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -43,7 +46,8 @@ def test_replicas_reduce_gloo():
         p.join(timeout=60)
         assert p.exitcode == 0
     for r in range(world):
-        elapsed, cands, cells = got[r]
+        elapsed, cands, cells, all_true, one_false = got[r]
         assert elapsed == pytest.approx(2.0)        # the slowest rank
         assert cands == pytest.approx(3000.0)       # all ranks' candidates
         assert cells == pytest.approx(1.5e7)
+        assert all_true is True and one_false is False
