@@ -65,6 +65,7 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--lane-words", type=int, default=12, help="serving: words per lane of the latency shapes")
     ap.add_argument("--slots", type=int, default=4, help="serving: batches in flight")
+    ap.add_argument("--max-batch", type=int, default=0, help="serving: candidates per batch (0: the server's default)")
     ap.add_argument("--no-graphs", action="store_true", help="serving: launch batches without CUDA graphs")
     ap.add_argument("--traceback", action="store_true",
                     help="time the traceback of the workload's candidates within --tb-bound x m")
@@ -591,7 +592,8 @@ def run_serving(args):
     rng = np.random.default_rng(5)
     sweep, same = [], True
     clocks = ClockSampler(0)
-    with mg.Server(ref, distance=DIST, slots=args.slots, lane_words=args.lane_words, graphs=not args.no_graphs) as srv:
+    with mg.Server(ref, distance=DIST, slots=args.slots, lane_words=args.lane_words, graphs=not args.no_graphs,
+                   max_batch_candidates=args.max_batch) as srv:
         clocks.start()
         for rate in rates:
             k = int(min(n_req, max(300, rate * 1.0 / mean_c)))  # about one second of load
