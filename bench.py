@@ -281,7 +281,10 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded)", "gcups": float(cells.sum() / t / 1e9),
-            "config": {"workload": WORKLOAD_NAMES[k], "distance": DIST, "window": "aligned"},
+            "config": {"workload": WORKLOAD_NAMES[k], "distance": DIST, "window": "aligned",
+                       "path": "the reference's CPU Myers (computeAllQueriesCPU)" if kind == "reference"
+                       else "CPU port of the reference algorithm",
+                       "l2": "host caches (CPU)", "parallelism": f"{threads} host threads"},
             "cpu_baseline": {"value": cps, "unit": "candidates/s", "cores": threads, "kind": kind,
                              "sample": f"each step: first {s.num_reads} reads ({len(w['cands'])} candidates) "
                                        f"of the workload, OpenMP over {threads} threads"},
