@@ -162,6 +162,23 @@ __device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t
 #ifndef MYERS_FMA_SHIFT_MAX_W
 #define MYERS_FMA_SHIFT_MAX_W 8  // plain-100b +1.7% (measured); no change on wider shapes
 #endif
+// where the FMA-pipe shifts apply besides the plain single-lane shapes:
+// single-lane shapes of the persistent kernel gain too (short reads on the
+// batched path, +1.7%); multi-lane shapes lose (8-word lanes of 1000-base
+// reads, -1.1%), all measured
+#ifndef MYERS_FMA_SHIFT_BATCHED
+#define MYERS_FMA_SHIFT_BATCHED 1
+#endif
+#ifndef MYERS_FMA_SHIFT_MULTI
+#define MYERS_FMA_SHIFT_MULTI 0
+#endif
+
+// FMA-pipe shifts for shape (W, MULTI) in the plain or the persistent kernel.
+template <int W, bool MULTI, bool PERSISTENT>
+__host__ __device__ constexpr bool fma_shift() {
+  return W <= MYERS_FMA_SHIFT_MAX_W && (!MULTI || MYERS_FMA_SHIFT_MULTI) &&
+         (!PERSISTENT || MYERS_FMA_SHIFT_BATCHED);
+}
 
 // (cur << 1) | (prev >> 31): the one-bit shift of a multi-word vector.
 // On the ALU pipe: one funnel shift. On the FMA pipe: multiply-high and
@@ -169,9 +186,9 @@ __device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t
 // instructions and latency in all, which only pays where many warps are
 // resident (narrow shapes). FMA for shapes of at most MYERS_FMA_SHIFT_MAX_W
 // words (MYERS_SHIFT_MODE=2: all shapes).
-template <int W>
+template <bool FS>
 __device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k) {
-  if constexpr (MYERS_SHIFT_MODE == 2 || W <= MYERS_FMA_SHIFT_MAX_W) {
+  if constexpr (MYERS_SHIFT_MODE == 2 || FS) {
     return cur * k.two + __umulhi(prev, k.two);
   } else {
     (void)k;
@@ -183,7 +200,7 @@ __device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k) {
 // horizontal delta (+1 / -1) entering the bottom row (Myers' block rule);
 // without, it is 0 (semi-global: row 0 of the DP is all zeros).
 // topP / topM return the unshifted top words (bit 31 = delta out of the top row).
-template <int W, bool HIN>
+template <int W, bool HIN, bool FS>
 __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (&Pv)[W], uint32_t (&Mv)[W],
                                              uint32_t inP, uint32_t inM, uint32_t& topP, uint32_t& topM, Mul k) {
   uint32_t e0 = eq[0];
@@ -202,8 +219,8 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
     const uint32_t xh = (s[j] ^ pv) | e;
     const uint32_t ph = mv | ~(xh | pv);
     const uint32_t mh = pv & xh;
-    const uint32_t phs = shl1<W>(php, ph, k);
-    const uint32_t mhs = shl1<W>(mhp, mh, k);
+    const uint32_t phs = shl1<FS>(php, ph, k);
+    const uint32_t mhs = shl1<FS>(mhp, mh, k);
     Pv[j] = mhs | ~(xv | phs);
     Mv[j] = phs & xv;
     php = ph;
@@ -216,7 +233,7 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
 // Eight columns of one text word, single-lane shapes. TAIL masks columns >= n.
 // Eight columns of one text word (codes 0..4 in its nibbles), single-lane
 // shapes. TAIL masks columns >= n.
-template <int W, bool TAIL, int UNR>
+template <int W, bool TAIL, int UNR, bool FS>
 __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                               uint32_t (&Mv)[W], uint32_t& sc, uint32_t& kmin,
                                               uint32_t colbase, uint32_t n, Mul k) {
@@ -228,7 +245,7 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
     uint32_t eq[W];
     load_eq<W, false>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
     uint32_t tp, tm;
-    myers_column<W, false>(eq, Pv, Mv, 0u, 0u, tp, tm, k);
+    myers_column<W, false, FS>(eq, Pv, Mv, 0u, 0u, tp, tm, k);
     sc = score_step(sc, tp, tm, k);
     const uint32_t key = sc + colbase + (uint32_t)u;
     if (!TAIL || colbase + (uint32_t)u < n) kmin = min(kmin, key);
@@ -239,7 +256,7 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
 // outside their candidate's columns (pipeline fill and drain, shorter
 // candidates); otherwise every lane with work is inside (steady state), and
 // lanes without work compute values nobody reads.
-template <int W, bool CHECKED, int UNR>
+template <int W, bool CHECKED, int UNR, bool FS>
 __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                              uint32_t (&Mv)[W], uint32_t& outP, uint32_t& outM, uint32_t& sc,
                                              uint32_t& kmin, uint32_t jbase, uint32_t n, bool work,
@@ -256,7 +273,7 @@ __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict_
     const uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1) * segmul;
     const uint32_t j = jbase + (uint32_t)u;  // wraps when negative
     if (!CHECKED || (work && j < n)) {
-      myers_column<W, true>(eq, Pv, Mv, inP, inM, outP, outM, k);
+      myers_column<W, true, FS>(eq, Pv, Mv, inP, inM, outP, outM, k);
       sc = score_step(sc, outP, outM, k);
       kmin = min(kmin, sc + j);
     }
@@ -328,7 +345,7 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
 // UNR: how far the 8 columns of a text word are unrolled -- fully for the
 // one-shape plain kernels; partly in the persistent kernel, whose code holds
 // every shape and would otherwise overflow the instruction cache.
-template <int W, bool MULTI, int UNR = 8>
+template <int W, bool MULTI, int UNR = 8, bool FS = false>
 __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
                                              uint32_t cnt, int L, uint32_t* __restrict__ wsmem, int lane) {
   using Lay = Layout<W, MULTI>;
@@ -388,11 +405,11 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
           const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
           lo = hi;
           hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
-          block8_single<W, false, UNR>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
+          block8_single<W, false, UNR, FS>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
         }
         if (c.n & 7u) {
           const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
-          block8_single<W, true, UNR>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
+          block8_single<W, true, UNR, FS>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
         }
         in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
       }
@@ -412,9 +429,9 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
         hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
         const uint32_t jbase = 8u * i - (uint32_t)l;
         if (8u * i + 1u >= (uint32_t)L && 8u * i + 8u <= n_min)
-          block8_multi<W, false, UNR>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
+          block8_multi<W, false, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
         else
-          block8_multi<W, true, UNR>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
+          block8_multi<W, true, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
       }
       if (work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
     }
@@ -450,7 +467,7 @@ __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __r
     if (t >= tiles) break;
     const uint32_t f = t * nseg;
     const uint32_t cnt = min((uint32_t)nseg, count - f);
-    process_tile<W, MULTI>(in, ids, first + f, cnt, L, wsmem, lane);
+    process_tile<W, MULTI, 8, fma_shift<W, MULTI, false>()>(in, ids, first + f, cnt, L, wsmem, lane);
   }
 }
 
@@ -546,10 +563,12 @@ template <int V>
 __device__ __forceinline__ void dispatch_one(const DevInputs& in, const uint32_t* ids, uint32_t f, uint32_t cnt,
                                              int L, uint32_t* wsmem, int lane) {
   if constexpr (V < kNumSingle) {
-    process_tile<V + 1, false, MYERS_BATCHED_UNROLL>(in, ids, f, cnt, L, wsmem, lane);
+    process_tile<V + 1, false, MYERS_BATCHED_UNROLL, fma_shift<V + 1, false, true>()>(in, ids, f, cnt, L, wsmem,
+                                                                                       lane);
   } else {
     if constexpr (kMultiW[V - kNumSingle] <= kBatchedMaxMultiW)
-      process_tile<kMultiW[V - kNumSingle], true, MYERS_BATCHED_UNROLL>(in, ids, f, cnt, L, wsmem, lane);
+      process_tile<kMultiW[V - kNumSingle], true, MYERS_BATCHED_UNROLL,
+                   fma_shift<kMultiW[V - kNumSingle], true, true>()>(in, ids, f, cnt, L, wsmem, lane);
   }
 }
 
