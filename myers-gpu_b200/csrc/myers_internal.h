@@ -92,7 +92,7 @@ struct DevInputs {
   int exact;
   // Multipliers the compiler cannot fold (set by set_multipliers): they keep
   // the per-column bookkeeping on the FMA pipe (see myers_kernels.cu).
-  uint32_t one, two, k16, mk16, p28, kb33, kb17;
+  uint32_t one, two, k16, mk16, p28, kb33, kb17, mn16;
 };
 
 inline void set_multipliers(DevInputs& in) {
@@ -103,6 +103,7 @@ inline void set_multipliers(DevInputs& in) {
   in.p28 = 1u << 28;
   in.kb33 = 33u * 4u * 4u;  // bytes between the bases of a PEQ group, 33 columns
   in.kb17 = 17u * 4u * 4u;  // ... 17 columns
+  in.mn16 = 0xFFFFFFF0u;    // -16
 }
 
 inline int variant_W(int v) { return v < kNumSingle ? v + 1 : kMultiW[v - kNumSingle]; }

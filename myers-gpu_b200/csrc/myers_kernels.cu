@@ -123,10 +123,31 @@ struct Mul {
   uint32_t k16, mk16;  // 1 << 16, -(1 << 16)
   uint32_t p28;        // 1 << 28: umulhi(x, p28) = x >> 4
   uint32_t kb33, kb17; // bytes between bases of a group for 33 / 17 columns
+  uint32_t mn16;       // -16
 };
 
 __device__ __forceinline__ Mul make_mul(const DevInputs& in) {
-  return Mul{in.one, in.two, in.k16, in.mk16, in.p28, in.kb33, in.kb17};
+  return Mul{in.one, in.two, in.k16, in.mk16, in.p28, in.kb33, in.kb17, in.mn16};
+}
+
+#ifndef MYERS_FMA_KEY
+#define MYERS_FMA_KEY 1
+#endif
+
+// The next text code (low nibble of t) and t shifted to the following one.
+// With MYERS_FMA_KEY both are FMA-pipe ops: the code is t - 16 * (t >> 4),
+// equal to t & 7 since sanitised codes are 0..4.
+__device__ __forceinline__ uint32_t next_code(uint32_t& t, Mul k) {
+#if MYERS_FMA_KEY
+  const uint32_t tn = __umulhi(t, k.p28);
+  const uint32_t code = tn * k.mn16 + t;
+  t = tn;
+  return code;
+#else
+  const uint32_t code = t & 7u;
+  t = __umulhi(t, k.p28);
+  return code;
+#endif
 }
 
 // Score key update for one column on the FMA pipe: the top row's Ph / Mh bit
@@ -136,6 +157,17 @@ __device__ __forceinline__ uint32_t score_step(uint32_t sc, uint32_t tp, uint32_
   const uint32_t hm = __umulhi(tm, k.two);
   sc = hp * k.k16 + sc;
   return hm * k.mk16 + sc;
+}
+
+// The same with the column folded in: sk holds score << 16 plus the column
+// and advances by one column per call -- the (score, column) key without an
+// ALU add.
+__device__ __forceinline__ uint32_t key_step(uint32_t sk, uint32_t tp, uint32_t tm, Mul k) {
+  const uint32_t hp = __umulhi(tp, k.two);
+  const uint32_t hm = __umulhi(tm, k.two);
+  const uint32_t up = hp * k.k16 + k.one;
+  sk = hm * k.mk16 + sk;
+  return up * k.one + sk;
 }
 
 // Bytes between the bases of a PEQ group for shape (W, MULTI).
@@ -240,15 +272,19 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
   const uint32_t kb = base_bytes<W, false>(k);
 #pragma unroll UNR
   for (int u = 0; u < 8; ++u) {
-    const uint32_t code = t & 7u;
-    t = __umulhi(t, k.p28);  // next nibble
+    const uint32_t code = next_code(t, k);
     uint32_t eq[W];
     load_eq<W, false>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
     uint32_t tp, tm;
     myers_column<W, false, FS>(eq, Pv, Mv, 0u, 0u, tp, tm, k);
+#if MYERS_FMA_KEY
+    sc = key_step(sc, tp, tm, k);  // sc: score key plus column
+    if (!TAIL || colbase + (uint32_t)u < n) kmin = min(kmin, sc);
+#else
     sc = score_step(sc, tp, tm, k);
     const uint32_t key = sc + colbase + (uint32_t)u;
     if (!TAIL || colbase + (uint32_t)u < n) kmin = min(kmin, key);
+#endif
   }
 }
 
@@ -264,19 +300,29 @@ __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict_
   const uint32_t kb = base_bytes<W, true>(k);
 #pragma unroll UNR
   for (int u = 0; u < 8; ++u) {
-    const uint32_t code = t & 7u;
-    t = __umulhi(t, k.p28);
+    const uint32_t code = next_code(t, k);
     uint32_t eq[W];
     load_eq<W, true>(reinterpret_cast<const uint32_t*>(slot + code * kb), eq);
     // the bottom lane of a segment takes no delta (segmul 0)
     const uint32_t inP = __shfl_up_sync(FULL_MASK, outP, 1) * segmul;
     const uint32_t inM = __shfl_up_sync(FULL_MASK, outM, 1) * segmul;
     const uint32_t j = jbase + (uint32_t)u;  // wraps when negative
+#if MYERS_FMA_KEY
+    // sc holds the key plus the step's column j; it advances every step
+    if (!CHECKED || (work && j < n)) {
+      myers_column<W, true, FS>(eq, Pv, Mv, inP, inM, outP, outM, k);
+      sc = key_step(sc, outP, outM, k);
+      kmin = min(kmin, sc);
+    } else {
+      sc = sc * k.one + k.one;
+    }
+#else
     if (!CHECKED || (work && j < n)) {
       myers_column<W, true, FS>(eq, Pv, Mv, inP, inM, outP, outM, k);
       sc = score_step(sc, outP, outM, k);
       kmin = min(kmin, sc + j);
     }
+#endif
   }
 }
 
@@ -394,6 +440,11 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
     }
     uint32_t sc = (uint32_t)rows << 16;  // score + p = rows at column -1
     uint32_t kmin = sc;                  // (score, column) = (m, 0) before any column
+#if MYERS_FMA_KEY
+    // the key counter: score << 16 plus the column, one column before the
+    // first (the lane's first step is column -l on multi-lane shapes)
+    sc -= 1u + (uint32_t)l;
+#endif
 
     if constexpr (!MULTI) {
       if (work) {
