@@ -272,3 +272,40 @@ def test_dropin_graph_replay(gpu, orc, workloads):
         finally:
             bufs.close()
             gpu.lib.myersSetMemoryBudget(0)
+
+
+def test_concurrent_contexts_on_two_streams(gpu, orc, workloads):
+    """Two contexts verifying different batches at the same time on two
+    streams (a plain launch whose warps take tiles from the context's counter,
+    and the persistent kernel on the other): each batch's results equal the
+    oracle's. Contexts share no device state."""
+    import torch
+    ref_words, ref_size, ws = workloads
+    ref = gpu.Reference(ref_words, ref_size)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1)).cuda()
+
+    jobs = []
+    for k, path in ((2, gpu.PATH_PLAIN), (3, gpu.PATH_BATCHED)):
+        w = ws[k]
+        n = len(w["cands"])
+        jobs.append(dict(w=w, path=path, ctx=gpu.Context(n), stream=torch.cuda.Stream(),
+                         d=(dev(w["peq"]), dev(w["qinfo"]), dev(w["cands"])),
+                         res=torch.empty(n * 8, dtype=torch.uint8, device="cuda")))
+    try:
+        for _ in range(2):  # twice: the counters start again at every launch
+            for j in jobs:
+                w, (d_peq, d_qi, d_c) = j["w"], j["d"]
+                j["ctx"].verify(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]),
+                                d_c.data_ptr(), len(w["cands"]), DIST, j["res"].data_ptr(), path=j["path"],
+                                stream=j["stream"].cuda_stream)
+            torch.cuda.synchronize()
+            for j in jobs:
+                w = j["w"]
+                got = j["res"].cpu().numpy().view(gpu.RES)
+                assert np.array_equal(got, orc.verify(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST))
+    finally:
+        for j in jobs:
+            j["ctx"].close()
+        ref.close()
