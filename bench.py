@@ -67,6 +67,8 @@ def parse_args():
     ap.add_argument("--slots", type=int, default=4, help="serving: batches in flight")
     ap.add_argument("--max-batch", type=int, default=0, help="serving: candidates per batch (0: the server's default)")
     ap.add_argument("--no-graphs", action="store_true", help="serving: launch batches without CUDA graphs")
+    ap.add_argument("--shape", type=int, default=0,
+                    help="verify every length bucket with multi-lane lanes of this many words (0: tuned shapes)")
     ap.add_argument("--traceback", action="store_true",
                     help="time the traceback of the workload's candidates within --tb-bound x m")
     ap.add_argument("--tb-bound", type=float, default=0.2, help="traceback: score bound as a fraction of m")
@@ -308,6 +310,15 @@ def run_ours(args):
 
     ref = mg.Reference(ref_words, ref_size)
     ctx = mg.Context(n_cands)
+    shape_note = None
+    if args.shape:
+        # one multi-lane shape per length bucket: lanes of args.shape words
+        v = [v for v, W, multi in mg.variants() if multi and W == args.shape]
+        if not v:
+            raise SystemExit(f"no multi-lane shape with {args.shape} words per lane")
+        for words in np.unique((lengths.astype(np.int64) + 31) // 32):
+            mg.set_shape_override(path, int(words), v[0], max(2, -(-int(words) // args.shape)))
+        shape_note = f"every bucket: lanes of {args.shape} words (override)"
 
     def dev(a):
         return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to("cuda")
@@ -417,7 +428,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD_NAMES[k], "candidates_per_gpu": n_cands, "distance": DIST,
                        "window": "aligned", "path": "batched" if path == mg.PATH_BATCHED else "plain",
                        "l2": "L2 flushed before every timed step (256 MiB write, untimed)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       **({"shapes": shape_note} if shape_note else {})},
             "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "3-input logic op probe (LOP3, 8 independent chains) in this run",
