@@ -90,11 +90,7 @@ def test_uniform_length_single_launch(gpu, orc, workloads):
     assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST))
 
 
-@pytest.mark.parametrize("variant_L", [(4, 2), (4, 9), (6, 6), (8, 4), (10, 3), (12, 3), (16, 2), (32, 2)])
-def test_every_multi_shape(gpu, orc, workloads, variant_L):
-    """Force each multi-lane variant (including L not dividing 32) on reads
-    of up to 1000 bases and compare with the oracle."""
-    W, L = variant_L
+def _forced_shape(gpu, orc, workloads, W, L, path):
     ref, ref_size, ws = workloads
     w = ws[3]
     v = [x for x, ww, multi in gpu.variants() if multi and ww == W][0]
@@ -102,12 +98,27 @@ def test_every_multi_shape(gpu, orc, workloads, variant_L):
     try:
         for wd in words:
             if W * L >= wd:
-                gpu.set_shape_override(gpu.PATH_PLAIN, wd, v, L)
-        res, _, _ = _run(gpu, ref, ref_size, w["peq"], w["qinfo"], w["cands"], gpu.WINDOW_ALIGNED, gpu.PATH_PLAIN)
+                gpu.set_shape_override(path, wd, v, L)
+        res, _, _ = _run(gpu, ref, ref_size, w["peq"], w["qinfo"], w["cands"], gpu.WINDOW_ALIGNED, path)
     finally:
         for wd in words:
-            gpu.set_shape_override(gpu.PATH_PLAIN, wd, -1)
+            gpu.set_shape_override(path, wd, -1)
     assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST))
+
+
+@pytest.mark.parametrize("variant_L", [(4, 2), (4, 9), (5, 7), (6, 6), (7, 5), (8, 4), (10, 3), (12, 3), (16, 2),
+                                       (32, 2)])
+def test_every_multi_shape(gpu, orc, workloads, variant_L):
+    """Force each multi-lane variant (including L not dividing 32) on reads
+    of up to 1000 bases in the plain kernel and compare with the oracle."""
+    _forced_shape(gpu, orc, workloads, *variant_L, gpu.PATH_PLAIN)
+
+
+@pytest.mark.parametrize("variant_L", [(4, 8), (5, 7), (6, 6), (7, 5), (8, 4), (10, 4), (12, 3), (16, 2)])
+def test_every_multi_shape_persistent(gpu, orc, workloads, variant_L):
+    """The same in the persistent kernel (the serving loop's latency shapes
+    run there): every multi-lane width it carries."""
+    _forced_shape(gpu, orc, workloads, *variant_L, gpu.PATH_BATCHED)
 
 
 def test_all_lengths_1_to_300(gpu, orc):
