@@ -372,8 +372,9 @@ typedef struct {
     int path;                    /* MYERS_PATH_* (default batched) */
     uint32_t maxQuerySize;       /* longest read accepted (0: 1024 bases) */
     uint32_t laneWords;          /* 0: throughput shapes; k > 0: spread a read of more than k
-                                    32-bit words over several lanes of >= k words each, which
-                                    cuts its time on the GPU (latency) for a few percent more work */
+                                    32-bit words over several lanes of at most k words each (the
+                                    cheapest such shape), which cuts its time on the GPU
+                                    (latency) for some more work */
     int useGraphs;               /* non-zero: capture each batch's copies and kernels and replay them
                                     as a CUDA graph (updated in place batch to batch) */
 } myersServerConfig_t;

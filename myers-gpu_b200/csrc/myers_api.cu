@@ -242,9 +242,9 @@ static void load_tuned_once() {
 }
 
 // lane_words > 0 asks for latency-oriented shapes: a query of more than
-// lane_words words is spread over ceil(words / W) lanes, W the smallest
-// multi-lane width >= lane_words (shorter per-candidate time, a few percent
-// more instructions).
+// lane_words words is spread over ceil(words / W) lanes of W <= lane_words
+// words, the cheapest such shape by the cost model (shorter per-candidate
+// time, some more instructions).
 static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
   load_tuned_once();
   {
