@@ -319,13 +319,25 @@ __global__ void __launch_bounds__(128) k_tb_forward(TbArgs a) {
     int hout = 0;
     uint32_t top = on ? 32u * g.tw : 0u;  // D at the top row, column 0 (last lane of the segment)
     const uint32_t x0 = r * W;            // the lane's first word
+    // The lane's text: its columns are consecutive bases from the window
+    // start, read one sanitised word at a time (the next word fetched ahead).
+    long long widx = on ? (long long)(g.start >> 3) : 0;
+    uint32_t nib = on ? (uint32_t)(g.start & 7ull) : 0u;
+    uint32_t tw = on ? sanitize_codes(ref_load(a.ref, widx, a.ref_words)) : 0u;
+    uint32_t tw_next = on ? ref_load(a.ref, widx + 1, a.ref_words) : 0u;
     for (uint32_t t = 0; t < steps; ++t) {
       int hin = __shfl_up_sync(FULL_MASK, hout, 1, S);
       if (r == 0) hin = 0;
       const int j = (int)t - (int)r;  // 0-based text base of this lane's column
       hout = 0;
       if (on && j >= 0 && (uint32_t)j < g.c1) {
-        const uint32_t code = ref_code(a.ref, g.start + (unsigned long long)j, a.ref_words);
+        const uint32_t code = (tw >> (4u * nib)) & 0xFu;
+        if (++nib == 8u) {
+          nib = 0u;
+          ++widx;
+          tw = sanitize_codes(tw_next);
+          tw_next = ref_load(a.ref, widx + 1, a.ref_words);
+        }
         hout = tb_column<W>(sm + code * W, Pv, Mv, hin, ph, mh);
         const uint32_t j1 = (uint32_t)j + 1u;
         if (r == g.L - 1u) top += (uint32_t)hout;
