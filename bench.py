@@ -19,19 +19,26 @@ JSON line (rank 0).
   roofline  the Myers kernel against the measured integer-ALU peak (3-input
             logic ops/s probed in this run): achieved = word-steps x 11 ops
             per launch / launch time
-  cpu_baseline  the reference's own CPU Myers (compiled from its sources into
-            oracle/_ref) on the host cores, on a bounded sample
+  parity    a seeded random 10% of the timed results against the reference's
+            own CPU Myers (computeAllQueriesCPU, compiled from its sources
+            into oracle/_ref), bit for bit
+  cpu_baseline  that same reference run: its candidates / its seconds on the
+            host cores
+  configs   (1 GPU, default workload) the other configurations, each with its
+            own timing, clocks, roofline fraction and reference parity sample:
+            plain-100b, batched-mixed (batched and plain, full size and a
+            110K-candidate batch), batched-long, and a short serving sweep
 
 --impl reference times the reference's own CPU implementation instead (the
 GPU path of the reference targets sm_20..sm_50 only).
 """
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -41,6 +48,7 @@ sys.path.insert(0, os.path.join(ROOT, "myers-gpu_b200"))
 
 DIST = 0.2
 OPS_PER_WORD_STEP = 11  # the fused recurrence: PEQ select + 10 logic/add/shift ops
+L2_NOTE = "L2 flushed before every timed step (256 MiB write, untimed)"
 
 WORKLOAD_NAMES = {
     1: "plain-100b: 16 Mbase ref, 100K reads x 100 b, 11 cand/read (1.1M candidates)",
@@ -49,6 +57,11 @@ WORKLOAD_NAMES = {
     4: "batched-long: 3.1 Gbase ref, 100K reads of 1000..10000 b, 1+Poisson(4) cand/read",
     5: "serving-mix: 3.1 Gbase ref, 300K requests of one read (100..1000 b) and 1..64 candidates",
 }
+# offered rates (candidates/s) of the serving sweep in the default line: the
+# low end and the region around the knee
+SERVING_RATES_SHORT = [1e6, 2e7, 5e7, 7e7, 7.8e7, 8.2e7, 8.6e7, 9e7, 9.5e7]
+SERVING_RATES_FULL = [1e4, 1e5, 1e6, 2e6, 5e6, 1e7, 2e7, 3e7, 4e7, 5e7, 6e7, 7e7, 7.5e7, 8e7, 8.2e7, 8.4e7, 8.6e7,
+                      8.8e7, 9e7, 9.2e7, 9.5e7, 1e8, 1.1e8]
 
 
 def parse_args():
@@ -60,13 +73,17 @@ def parse_args():
     ap.add_argument("--path", default=None, choices=["plain", "batched"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the workload's reads (tests)")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample budget")
+    ap.add_argument("--parity-frac", type=float, default=0.1,
+                    help="fraction of the timed results checked against the reference's CPU Myers")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="no reference parity / CPU baseline run")
+    ap.add_argument("--no-configs", action="store_true", help="only the selected workload (no other configurations)")
     ap.add_argument("--lane-words", type=int, default=12, help="serving: words per lane of the latency shapes")
     ap.add_argument("--slots", type=int, default=4, help="serving: batches in flight")
     ap.add_argument("--max-batch", type=int, default=0, help="serving: candidates per batch (0: the server's default)")
     ap.add_argument("--no-graphs", action="store_true", help="serving: launch batches without CUDA graphs")
+    ap.add_argument("--cutoff", type=float, default=None,
+                    help="Ukkonen's cut-off: report minima above (uint32)(m * CUTOFF) as no match, skipping rows")
     ap.add_argument("--shape", type=int, default=0,
                     help="verify every length bucket with multi-lane lanes of this many words (0: tuned shapes)")
     ap.add_argument("--traceback", action="store_true",
@@ -202,53 +219,143 @@ def all_ranks_true(dist, flag, device="cuda"):
     return bool(t.item())
 
 
-def make_inputs(mg, k, scale, seed_offset, num_reads=None):
-    s = mg.workload_spec(k, scale=scale)
+_REF_CACHE = {}
+
+
+def reference_words(ms, k):
+    """The packed synthetic reference of workload k: 16 Mbases for plain-100b,
+    one shared 3.1 Gbase reference for the others (generated once)."""
+    s = ms.workload_spec(k)
+    key = (s.ref_size, 1000 + (s.seed if k == 1 else 0))
+    if key not in _REF_CACHE:
+        _REF_CACHE[key] = ms.make_reference(*key)
+    return _REF_CACHE[key], int(s.ref_size)
+
+
+def make_inputs(ms, k, scale, seed_offset, num_reads=None):
+    s = ms.workload_spec(k, scale=scale)
     s.seed += 7919 * seed_offset
     if num_reads is not None:
         s.num_reads = min(s.num_reads, num_reads)
-    ref_size = s.ref_size
-    ref_words = mg.make_reference(ref_size, 1000 + (s.seed if k == 1 else 0))
-    w = mg.make_workload(s, ref_words)
+    ref_words, ref_size = reference_words(ms, k)
+    w = ms.make_workload(s, ref_words)
     return s, ref_words, ref_size, w
 
 
-def cpu_baseline(mg, k, args, full_cands):
-    """Reference CPU Myers (oracle/_ref) on a bounded sample of the workload."""
+def write_ref_file(tmp, ref_words, ref_size):
+    """The reference as a .4bits.ref file (u32 words, u32 bases, words), the
+    format the drop-in initMyers loads."""
+    fn = os.path.join(tmp, f"bench.{ref_size}.4bits.ref")
+    if not os.path.exists(fn):
+        with open(fn, "wb") as f:
+            f.write(np.array([len(ref_words), ref_size], dtype=np.uint32).tobytes())
+            ref_words.tofile(f)
+    return fn
+
+
+def workload_units(ms, w):
+    cells, word_steps = ms.cells(w["qinfo"], w["cands"], DIST)
+    return float(cells.sum()), float(word_steps.sum())
+
+
+def device_run(mg, ref, w, path, steps, warmup, local=0, dist=None, cutoff=None):
+    """Time `steps` verification passes of workload w (inputs resident in HBM)
+    with CUDA events on the launching stream, L2 flushed before every step,
+    clocks sampled during the timed region. Returns per-step milliseconds, the
+    last step's results, the launches per step and the clock record."""
+    import torch
+    n = len(w["cands"])
+    ctx = mg.Context(n)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to("cuda")
+
+    d_peq, d_qi, d_c = dev(w["peq"]), dev(w["qinfo"]), dev(w["cands"])
+    d_res = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    lengths = w["qinfo"]["size"]
+    lo, hi = int(lengths.min()), int(lengths.max())
+
+    def step():
+        ctx.verify(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(), n, DIST,
+                   d_res.data_ptr(), path=path, stream=stream.cuda_stream, min_size=lo, max_size=hi, cutoff=cutoff)
+
+    try:
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        launches = ctx.launches()
+        clocks = ClockSampler(local)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        clocks.start()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            step()
+            b.record(stream)
+        clocks.poke()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        del flush
+        if dist is not None:
+            dist.barrier()
+        step_ms = [a.elapsed_time(b) for a, b in evs]
+        res = d_res.cpu().numpy().view(mg.RES).copy()
+    finally:
+        ctx.close()
+        del d_peq, d_qi, d_c, d_res
+        torch.cuda.empty_cache()
+    return {"step_ms": step_ms, "res": res, "launches": launches, "clocks": clk}
+
+
+def reference_parity(w, res, ref_words, ref_size, frac, seed, threads, padded=None, cutoff=None):
+    """Check a seeded random fraction of the results against the reference's
+    own CPU Myers (computeAllQueriesCPU of
+    src-integration/myers-reorderBuffer-padding.c:178-208, compiled into
+    oracle/_ref; reads beyond its 4096-base cap through its computeMyers,
+    :97-176), or the restated oracle where oracle/_ref is not built. Returns
+    (parity record, CPU rate record of that same run)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    threads = host_threads()
-    kind = "reference" if orc.have_reference() else "port"
+    n = len(w["cands"])
+    k = max(1, min(n, int(math.ceil(frac * n))))
+    idx = np.arange(n) if k >= n else np.sort(np.random.default_rng(seed).choice(n, size=k, replace=False))
+    sub = np.ascontiguousarray(w["cands"][idx])
+    if orc.have_reference():
+        expect, sec = orc.reference_verify_aligned(w["peq"], w["qinfo"], sub, ref_words, ref_size, DIST,
+                                                   nthreads=threads, padded=padded)
+        kind, who = "reference", "the reference's computeAllQueriesCPU (oracle/_ref)"
+    else:
+        t = time.perf_counter()
+        expect = orc.verify(w["peq"], w["qinfo"], sub, ref_words, ref_size, DIST, nthreads=threads)
+        sec = time.perf_counter() - t
+        kind, who = "port", "the restated oracle (oracle/myers_oracle.c)"
+    if cutoff is not None:
+        expect = orc.apply_cutoff(expect, w["qinfo"], sub, cutoff)
+    mism = int(np.count_nonzero(res[idx] != expect))
+    parity = {"candidates": int(k), "fraction": k / n, "oracle": who, "bit_exact": mism == 0, "mismatches": mism}
+    m = w["qinfo"]["size"][sub["query"]].astype(np.float64)
+    f = np.float32(1.0) + np.float32(2.0) * np.float32(DIST)
+    wb = np.floor(m.astype(np.float32) * f).astype(np.float64)
+    cells = float((m * 8 * (np.floor(wb / 8) + np.where(wb % 8 != 0, 2, 1))).sum())
+    what = "all" if k >= n else f"a seeded random {100 * k / n:.0f}% ({k})"
+    cpu = {"value": k / sec, "unit": "candidates/s", "cores": threads, "kind": kind, "gcups": cells / sec / 1e9,
+           "sample": f"{what} of the {n} candidates of the same workload, {sec:.1f} s, OpenMP over {threads} threads"}
+    return parity, cpu
 
-    def run(w, ref_words, ref_size):
-        if kind == "reference":
-            res, sec = orc.reference_verify_aligned(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST,
-                                                    nthreads=threads)
-        else:
-            t = time.perf_counter()
-            orc.verify(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST, nthreads=threads)
-            sec = time.perf_counter() - t
-        return sec
 
-    # probe with a few reads, then size the sample to the time budget
-    total_reads = mg.workload_spec(k, scale=args.scale).num_reads
-    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0, num_reads=max(1, 2000 // (10 if k in (2, 4) else 1)))
-    sec = max(run(w, ref_words, ref_size), 1e-4)
-    per_read = sec / len(w["qinfo"])
-    n_reads = int(max(len(w["qinfo"]), min(total_reads, args.cpu_seconds / per_read)))
-    s.num_reads = n_reads
-    w = mg.make_workload(s, ref_words)
-    sec = run(w, ref_words, ref_size)
-    cps = len(w["cands"]) / sec
-    cells, _ = mg.cells(w["qinfo"], w["cands"], DIST)
-    return {"value": cps, "unit": "candidates/s", "cores": threads, "kind": kind,
-            "gcups": float(cells.sum() / sec / 1e9),
-            "sample": f"first {n_reads} reads ({len(w['cands'])} candidates) of the same seeded workload, "
-                      f"{sec:.1f} s of CPU time, OpenMP over {threads} threads"}
+def roofline(peak, word_steps, kernel_s):
+    achieved = word_steps * OPS_PER_WORD_STEP / kernel_s
+    return {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
+            "frac": achieved / peak}
 
 
 def run_reference(args):
-    import myersgpu as mg
+    import myerssynth as ms  # the generator only: no CUDA library in this process
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -259,37 +366,44 @@ def run_reference(args):
     threads = host_threads()
     kind = "reference" if orc.have_reference() else "port"
     per_step = max(1.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
-    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0, num_reads=max(1, 2000 // (10 if k in (2, 4) else 1)))
+    s, ref_words, ref_size, w = make_inputs(ms, k, args.scale, 0, num_reads=max(1, 2000 // (10 if k in (2, 4) else 1)))
+    padded = orc.pad_reference(ref_words) if kind == "reference" else None
 
     def run(w):
         if kind == "reference":
             return orc.reference_verify_aligned(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST,
-                                                nthreads=threads)[1]
+                                                nthreads=threads, padded=padded)[1]
         t = time.perf_counter()
         orc.verify(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST, nthreads=threads)
         return time.perf_counter() - t
 
     sec = max(run(w), 1e-4)
-    total_reads = mg.workload_spec(k, scale=args.scale).num_reads
+    full = ms.workload_spec(k, scale=args.scale)
+    total_reads = full.num_reads
+    full_cands = len(ms.make_workload(full, ref_words)["cands"])
     s.num_reads = int(max(len(w["qinfo"]), min(total_reads, per_step / (sec / len(w["qinfo"])))))
-    w = mg.make_workload(s, ref_words)
+    w = ms.make_workload(s, ref_words)
     for _ in range(args.warmup):
         run(w)
     times = [run(w) for _ in range(args.steps)]
     t = float(np.mean(times))
     cps = len(w["cands"]) / t
-    cells, _ = mg.cells(w["qinfo"], w["cands"], DIST)
+    cells, _ = ms.cells(w["qinfo"], w["cands"], DIST)
     line = {"impl": "reference", "metric": "candidates/s", "value": cps, "unit": "candidates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded)", "gcups": float(cells.sum() / t / 1e9),
-            "config": {"workload": WORKLOAD_NAMES[k], "distance": DIST, "window": "aligned",
+            "config": {"workload": WORKLOAD_NAMES[k], "candidates_per_gpu": full_cands, "distance": DIST,
+                       "window": "aligned",
                        "path": "the reference's CPU Myers (computeAllQueriesCPU)" if kind == "reference"
                        else "CPU port of the reference algorithm",
-                       "l2": "host caches (CPU)", "parallelism": f"{threads} host threads"},
+                       "l2": "host caches (CPU)", "parallelism": f"{threads} host threads",
+                       "sample_candidates_per_step": len(w["cands"]),
+                       "sample_fraction": len(w["cands"]) / full_cands},
             "cpu_baseline": {"value": cps, "unit": "candidates/s", "cores": threads, "kind": kind,
-                             "sample": f"each step: first {s.num_reads} reads ({len(w['cands'])} candidates) "
-                                       f"of the workload, OpenMP over {threads} threads"},
+                             "sample": f"each step: first {s.num_reads} reads ({len(w['cands'])} candidates, "
+                                       f"{100 * len(w['cands']) / full_cands:.1f}% of the workload), "
+                                       f"OpenMP over {threads} threads"},
             "e2e": {"value": cps, "unit": "candidates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -298,18 +412,17 @@ def run_ours(args):
     import torch
 
     import myersgpu as mg
+    import myerssynth as ms
     world, rank, local, dist = dist_setup(args)
     torch.cuda.set_device(local)
     k = args.workload
     path = {"plain": mg.PATH_PLAIN, "batched": mg.PATH_BATCHED}[args.path or ("batched" if k in (3, 4, 5) else "plain")]
-    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, rank)
+    s, ref_words, ref_size, w = make_inputs(ms, k, args.scale, rank)
     n_cands = len(w["cands"])
     lengths = w["qinfo"]["size"]
-    cells, word_steps = mg.cells(w["qinfo"], w["cands"], DIST)
-    ws_total = float(word_steps.sum())
+    cells, ws_total = workload_units(ms, w)
 
     ref = mg.Reference(ref_words, ref_size)
-    ctx = mg.Context(n_cands)
     shape_note = None
     if args.shape:
         # one multi-lane shape per length bucket: lanes of args.shape words
@@ -320,65 +433,21 @@ def run_ours(args):
             mg.set_shape_override(path, int(words), v[0], max(2, -(-int(words) // args.shape)))
         shape_note = f"every bucket: lanes of {args.shape} words (override)"
 
-    def dev(a):
-        return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).to("cuda")
-
-    d_peq, d_qi, d_c = dev(w["peq"]), dev(w["qinfo"]), dev(w["cands"])
-    d_res = torch.empty(n_cands * 8, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream()
-    sp = stream.cuda_stream
-    lo, hi = int(lengths.min()), int(lengths.max())
-
-    def step():
-        ctx.verify(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(), n_cands,
-                   DIST, d_res.data_ptr(), path=path, stream=sp, min_size=lo, max_size=hi)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    launches_per_step = ctx.launches()
-
-    clocks = ClockSampler(local)
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    # L2 is flushed (a 256 MiB write, outside the events) before every timed step
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    clocks.start()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for a, b in evs:
-        flush.zero_()
-        a.record(stream)
-        step()
-        b.record(stream)
-    clocks.poke()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    del flush
-    if dist is not None:
-        dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
+    run = device_run(mg, ref, w, path, args.steps, args.warmup, local, dist, args.cutoff)
+    step_ms, res, clk = run["step_ms"], run["res"], run["clocks"]
     elapsed = sum(step_ms) / 1e3
     if dist is not None:
-        elapsed, all_cands, all_cells = reduce_over_ranks(dist, elapsed, n_cands, cells.sum(), "cuda")
+        elapsed, all_cands, all_cells = reduce_over_ranks(dist, elapsed, n_cands, cells, "cuda")
     else:
-        all_cands, all_cells = float(n_cands), float(cells.sum())
+        all_cands, all_cells = float(n_cands), cells
     value = all_cands * args.steps / elapsed
     gcups = all_cells * args.steps / elapsed / 1e9
-
-    # parity spot check of the timed output against the oracle (a sample)
-    res = d_res.cpu().numpy().view(mg.RES)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
-    idx = np.random.default_rng(rank).choice(n_cands, size=min(2000, n_cands), replace=False)
-    sub = w["cands"][idx]
-    expect = orc.verify(w["peq"], w["qinfo"], sub, ref_words, ref_size, DIST)
-    parity = bool(np.array_equal(res[idx], expect))
 
     # roofline: the dominant kernel is the whole step on the plain single-launch path
     peak = mg.probe_int_peak(4000)
     kernel_s = float(np.mean(step_ms)) / 1e3
-    achieved = ws_total * OPS_PER_WORD_STEP / kernel_s
+    roof = roofline(peak, ws_total, kernel_s)
+    _, word_steps = ms.cells(w["qinfo"], w["cands"], DIST)
     hbm_bytes = float(len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * (16 + 8)
                       + (word_steps / np.ceil(w["qinfo"]["size"][w["cands"]["query"]] / 32) / 2).sum())
     peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -386,13 +455,18 @@ def run_ours(args):
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"traffic_workload{k}.json")
     if os.path.exists(prof):
-        t = json.load(open(prof))
-        traffic = t["dram_bytes_per_candidate"] * n_cands
+        traffic = json.load(open(prof))["dram_bytes_per_candidate"] * n_cands
+    roof.update({"traffic": traffic,
+                 "peak_source": "3-input logic op probe (LOP3, 8 independent chains) in this run",
+                 "ops_per_word_step": OPS_PER_WORD_STEP,
+                 "hbm": {"achieved_gbs": hbm_bytes / kernel_s / 1e9, "peak_gbs": hbm_peak,
+                         "frac": hbm_bytes / kernel_s / 1e9 / hbm_peak}})
 
+    tmp = tempfile.TemporaryDirectory()
     # end to end through the drop-in API
     e2e = None
-    if not args.no_e2e:
-        e2e = run_e2e(mg, args, ref_words, ref_size, w, path, dist)
+    if not args.no_e2e and args.cutoff is None:
+        e2e = run_e2e(mg, args, write_ref_file(tmp.name, ref_words, ref_size), ref_size, w, path, dist)
         if "_results" in e2e:
             e2e["results_equal_device"] = bool(np.array_equal(e2e.pop("_results"), res))
         if dist is not None:
@@ -410,15 +484,35 @@ def run_ours(args):
                 e2e["results_equal_device"] = same
             else:
                 e2e = {"value": None, "unit": "candidates/s", "note": "a rank's buffers were too small"}
-    if dist is not None:
-        parity = all_ranks_true(dist, parity)
 
+    # parity of the timed results: 1 GPU against the reference's own CPU Myers
+    # on a seeded 10% (its time is the CPU baseline); N GPUs, where all ranks
+    # share the host, a 2,000-candidate sample per rank against the restated oracle
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(mg, k, args, n_cands)
+    threads = host_threads()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    padded = orc.pad_reference(ref_words) if orc.have_reference() else None
+    if world == 1 and not args.no_cpu:
+        parity, cpu = reference_parity(w, res, ref_words, ref_size, args.parity_frac, 11, threads, padded,
+                                       args.cutoff)
+    else:
+        idx = np.random.default_rng(rank).choice(n_cands, size=min(2000, n_cands), replace=False)
+        expect = orc.verify(w["peq"], w["qinfo"], w["cands"][idx], ref_words, ref_size, DIST)
+        if args.cutoff is not None:
+            expect = orc.apply_cutoff(expect, w["qinfo"], w["cands"][idx], args.cutoff)
+        ok = bool(np.array_equal(res[idx], expect))
+        if dist is not None:
+            ok = all_ranks_true(dist, ok)
+        parity = {"candidates": int(len(idx)) * world, "fraction": len(idx) / n_cands,
+                  "oracle": "the restated oracle (oracle/myers_oracle.c)", "bit_exact": ok}
+    del w, res
 
-    ctx.close()
+    configs = None
+    if rank == 0 and world == 1 and k == 2 and not args.no_configs and args.scale == 1.0 and args.cutoff is None:
+        configs = run_configs(mg, ms, args, ref, peak, tmp.name, threads, padded)
     ref.close()
+    tmp.cleanup()
     if rank == 0:
         line = {
             "metric": "candidates/s", "value": value, "unit": "candidates/s", "n_gpus": world, "steps": args.steps,
@@ -427,25 +521,134 @@ def run_ours(args):
             "gcups": gcups,
             "config": {"workload": WORKLOAD_NAMES[k], "candidates_per_gpu": n_cands, "distance": DIST,
                        "window": "aligned", "path": "batched" if path == mg.PATH_BATCHED else "plain",
-                       "l2": "L2 flushed before every timed step (256 MiB write, untimed)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       **({"shapes": shape_note} if shape_note else {})},
-            "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": "3-input logic op probe (LOP3, 8 independent chains) in this run",
-                         "ops_per_word_step": OPS_PER_WORD_STEP,
-                         "hbm": {"achieved_gbs": hbm_bytes / kernel_s / 1e9, "peak_gbs": hbm_peak,
-                                 "frac": hbm_bytes / kernel_s / 1e9 / hbm_peak}},
-            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": launches_per_step * args.steps,
-            "parity_sample": {"candidates": int(len(idx)), "bit_exact": parity},
+                       "l2": L2_NOTE, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       **({"shapes": shape_note} if shape_note else {}),
+                       **({"cutoff": args.cutoff} if args.cutoff is not None else {})},
+            "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": run["launches"] * args.steps,
+            "parity_sample": parity,
         }
+        if configs is not None:
+            line["configs"] = configs
+            line["north_star"] = north_star_summary(value, configs)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
 
-def run_e2e(mg, args, ref_words, ref_size, w, path, dist=None):
+def config_record(mg, ms, ref, w, path, steps, warmup, peak, ref_words, ref_size, threads, padded, parity_frac,
+                  seed):
+    """One configuration's figures: device-resident candidates/s with its
+    clocks, the roofline fraction, and a reference parity sample whose time
+    is the CPU baseline."""
+    n = len(w["cands"])
+    cells, ws = workload_units(ms, w)
+    r = device_run(mg, ref, w, path, steps, warmup)
+    t = float(np.mean(r["step_ms"])) / 1e3
+    rec = {"path": "batched" if path == mg.PATH_BATCHED else "plain", "candidates": n, "value": n / t,
+           "unit": "candidates/s", "ms_per_step": t * 1e3, "steps": steps, "warmup": warmup, "gcups": cells / t / 1e9,
+           "roofline_frac": roofline(peak, ws, t)["frac"], "launches_per_step": r["launches"], "clocks": r["clocks"]}
+    if parity_frac > 0:
+        rec["parity_sample"], rec["cpu_baseline"] = reference_parity(w, r["res"], ref_words, ref_size, parity_frac,
+                                                                     seed, threads, padded)
+    return rec, r["res"]
+
+
+def run_configs(mg, ms, args, ref3, peak, tmp, threads, padded3):
+    """The benchmark's other configurations, each on the same GPU in this run:
+    plain-100b (with its e2e), batched-mixed on both paths at full size and at
+    110K candidates (with the batched path's e2e), batched-long on both paths,
+    and a short serving sweep. Steps per configuration are capped so the whole
+    line stays within a few minutes."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    steps, warmup = min(args.steps, 10), min(args.warmup, 3)
+    out = {}
+
+    # plain-100b: its own 16 Mbase reference; all of its candidates checked
+    _, rw1, rs1, w1 = make_inputs(ms, 1, 1.0, 0)
+    ref1 = mg.Reference(rw1, rs1)
+    try:
+        rec, res = config_record(mg, ms, ref1, w1, mg.PATH_PLAIN, max(steps, 20), warmup, peak, rw1, rs1, threads,
+                                 orc.pad_reference(rw1) if padded3 is not None else None, 1.0, 101)
+        e2e = run_e2e(mg, argparse.Namespace(steps=steps, warmup=warmup), write_ref_file(tmp, rw1, rs1), rs1, w1,
+                      mg.PATH_PLAIN)
+        if "_results" in e2e:
+            e2e["results_equal_device"] = bool(np.array_equal(e2e.pop("_results"), res))
+        rec["e2e"] = e2e
+    finally:
+        ref1.close()
+    out["plain-100b"] = {"workload": WORKLOAD_NAMES[1], **rec}
+    del w1, res
+
+    rw, rs = reference_words(ms, 3)
+    fn = write_ref_file(tmp, rw, rs)
+    # batched-mixed at full size, both paths
+    _, _, _, w3 = make_inputs(ms, 3, 1.0, 0)
+    b, resb = config_record(mg, ms, ref3, w3, mg.PATH_BATCHED, steps, warmup, peak, rw, rs, threads, padded3,
+                            args.parity_frac, 303)
+    e2e = run_e2e(mg, argparse.Namespace(steps=steps, warmup=warmup), fn, rs, w3, mg.PATH_BATCHED)
+    if "_results" in e2e:
+        e2e["results_equal_device"] = bool(np.array_equal(e2e.pop("_results"), resb))
+    b["e2e"] = e2e
+    p, resp = config_record(mg, ms, ref3, w3, mg.PATH_PLAIN, steps, warmup, peak, rw, rs, threads, padded3, 0.0, 0)
+    p["results_equal_batched"] = bool(np.array_equal(resp, resb))
+    out["batched-mixed"] = {"workload": WORKLOAD_NAMES[3], "batched": b, "plain": p,
+                            "batched_over_plain": b["value"] / p["value"]}
+    del w3, resb, resp
+
+    # batched-mixed, a 110K-candidate batch (0.5% of the reads): where one
+    # persistent launch and per-shape launches differ most
+    _, _, _, ws3 = make_inputs(ms, 3, 0.005, 0)
+    bs, resb = config_record(mg, ms, ref3, ws3, mg.PATH_BATCHED, max(steps, 20), warmup, peak, rw, rs, threads,
+                             padded3, 1.0, 304)
+    ps, resp = config_record(mg, ms, ref3, ws3, mg.PATH_PLAIN, max(steps, 20), warmup, peak, rw, rs, threads,
+                             padded3, 0.0, 0)
+    ps["results_equal_batched"] = bool(np.array_equal(resp, resb))
+    out["batched-mixed-110k"] = {"workload": WORKLOAD_NAMES[3] + ", first 0.5% of the reads", "batched": bs,
+                                 "plain": ps, "batched_over_plain": bs["value"] / ps["value"]}
+    del ws3, resb, resp
+
+    # batched-long, both paths
+    _, _, _, w4 = make_inputs(ms, 4, 1.0, 0)
+    b4, resb = config_record(mg, ms, ref3, w4, mg.PATH_BATCHED, min(steps, 5), warmup, peak, rw, rs, threads,
+                             padded3, args.parity_frac, 404)
+    p4, resp = config_record(mg, ms, ref3, w4, mg.PATH_PLAIN, min(steps, 5), warmup, peak, rw, rs, threads,
+                             padded3, 0.0, 0)
+    p4["results_equal_batched"] = bool(np.array_equal(resp, resb))
+    out["batched-long"] = {"workload": WORKLOAD_NAMES[4], "batched": b4, "plain": p4,
+                           "batched_over_plain": b4["value"] / p4["value"]}
+    del w4, resb, resp
+
+    # serving: a short sweep around the knee
+    out["serving"] = serving_sweep(mg, ms, args, ref3, rw, rs, SERVING_RATES_SHORT, steps=min(steps, 5),
+                                   warmup=warmup, threads=threads, padded=padded3)
+    return out
+
+
+def north_star_summary(value_plain_1000b, configs):
+    """The targets, as measured in this line."""
+    sv = configs["serving"]
+    records = []  # every per-path record of every configuration
+    for c in configs.values():
+        records += [c[p] for p in ("batched", "plain") if p in c] or [c]
+    samples = [r["parity_sample"] for r in records if "parity_sample" in r]
+    same = ([r["results_equal_batched"] for r in records if "results_equal_batched" in r]
+            + [r["e2e"]["results_equal_device"] for r in records if "results_equal_device" in (r.get("e2e") or {})]
+            + [sv["results_equal_to_batched"]])
+    return {
+        "batched_over_plain_mixed_full": configs["batched-mixed"]["batched_over_plain"],
+        "batched_over_plain_mixed_110k": configs["batched-mixed-110k"]["batched_over_plain"],
+        "batched_over_plain_long": configs["batched-long"]["batched_over_plain"],
+        "serving_frac_of_batched_at_p99_le_5ms": sv["served_frac_of_batched"],
+        "serving_p99_ms": (sv["best"] or {}).get("p99_ms"),
+        "reference_parity_candidates": int(sum(p["candidates"] for p in samples)),
+        "bit_exact_everywhere": all(p["bit_exact"] for p in samples) and all(same),
+        "plain_1000b_cand_s": value_plain_1000b,
+    }
+
+
+def run_e2e(mg, args, ref_file, ref_size, w, path, dist=None):
     """The metric through the drop-in API from pinned host buffers: every
     step copies its inputs in and its results out. When the resident
     reference is much larger than L2 (3.1 Gbase: 1.55 GB), steps stream
@@ -454,16 +657,11 @@ def run_e2e(mg, args, ref_words, ref_size, w, path, dist=None):
     one at a time on one buffer, with L2 flushed between them."""
     n_cands = len(w["cands"])
     nb = 2 if ref_size // 2 > (1 << 30) else 1
-    with tempfile.TemporaryDirectory() as tmp:
-        fn = os.path.join(tmp, "bench.4bits.ref")
-        with open(fn, "wb") as f:
-            f.write(np.array([len(ref_words), ref_size], dtype=np.uint32).tobytes())
-            ref_words.tofile(f)
-        need = len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * 32
-        mg.lib.myersSetMemoryBudget(nb * (int(need * 1.3) + (64 << 20)))
-        avg = int(w["qinfo"]["size"].mean())
-        cpq = max(1, n_cands // max(1, len(w["qinfo"])))
-        bufs = mg.Buffers(fn, num_buffers=nb, avg_query_size=avg, cands_per_query=cpq)
+    need = len(w["peq"]) * 80 + len(w["qinfo"]) * 8 + n_cands * 32
+    mg.lib.myersSetMemoryBudget(nb * (int(need * 1.3) + (64 << 20)))
+    avg = int(w["qinfo"]["size"].mean())
+    cpq = max(1, n_cands // max(1, len(w["qinfo"])))
+    bufs = mg.Buffers(ref_file, num_buffers=nb, avg_query_size=avg, cands_per_query=cpq)
     try:
         bufs.set_path(path)
         for b in range(nb):
@@ -513,7 +711,7 @@ def run_e2e(mg, args, ref_words, ref_size, w, path, dist=None):
         how = ("two buffers in flight: step i sends on buffer i % 2 once that buffer's step i-2 is received"
                if nb == 2 else "one buffer, one step at a time, L2 flushed between steps")
         return {"value": n_cands * args.steps / el, "unit": "candidates/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(n_cands * 8), "buffers": nb,
+                "d2h_bytes_per_step": int(n_cands * 8), "buffers": nb, "steps": args.steps,
                 "api": "initMyers buffers: fill pinned host buffers (untimed), then sendMyersBuffer + "
                        "receiveMyersBuffer per step (H2D, kernels, D2H timed on the host clock); " + how,
                 "_results": res}
@@ -522,25 +720,18 @@ def run_e2e(mg, args, ref_words, ref_size, w, path, dist=None):
         mg.lib.myersSetMemoryBudget(0)
 
 
-def run_serving(args):
-    """Workload 5: open-loop Poisson arrivals of requests (one read of 100..1000
-    bases and 1..64 candidates) into the serving loop, at a sweep of offered
-    rates; p50/p99 latency (arrival -> results on the host) and throughput per
-    rate, beside the batched kernel's throughput on the same requests."""
+def serving_sweep(mg, ms, args, ref, ref_words, ref_size, rates, steps, warmup, threads, padded=None):
+    """Open-loop Poisson arrivals of requests (one read of 100..1000 bases and
+    1..64 candidates) into the serving loop at the given offered rates; p50/p99
+    latency (arrival -> results on the host) and throughput per rate, beside
+    the batched kernel's throughput on the same requests as one batch."""
     import torch
-
-    import myersgpu as mg
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    if rank != 0:
-        return
-    torch.cuda.set_device(0)
     # a pool of 300K requests (~9.8M candidates): ~0.1 s of load at the top rates
-    s, ref_words, ref_size, w = make_inputs(mg, 5, 3.0 * args.scale, 0)
+    s = ms.workload_spec(5, scale=3.0 * args.scale)
+    w = ms.make_workload(s, ref_words)
     off = np.concatenate([[0], np.cumsum(w["ncands"])]).astype(np.uint32)
     n_req, n_cands = len(w["qinfo"]), len(w["cands"])
     mean_c = n_cands / n_req
-    ref = mg.Reference(ref_words, ref_size)
 
     # batched kernel on all requests at once, inputs resident (the comparison point)
     ctx = mg.Context(n_cands)
@@ -556,16 +747,16 @@ def run_serving(args):
         ctx.verify(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), n_req, d_c.data_ptr(), n_cands, DIST,
                    d_res.data_ptr(), path=mg.PATH_BATCHED, stream=st.cuda_stream, min_size=100, max_size=1000)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(st)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     b.record(st)
     torch.cuda.synchronize()
-    batched_cps = n_cands * args.steps / (a.elapsed_time(b) / 1e3)
-    batched_res = d_res.cpu().numpy().view(mg.RES)
+    batched_cps = n_cands * steps / (a.elapsed_time(b) / 1e3)
+    batched_res = d_res.cpu().numpy().view(mg.RES).copy()
     # the same, with the shapes the server picks (latency shapes), to split the
     # serving gap into shape cost and serving-loop cost
     same_cps = None
@@ -591,19 +782,17 @@ def run_serving(args):
         for _ in range(2):
             step()
         a.record(st)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step()
         b.record(st)
         torch.cuda.synchronize()
-        same_cps = n_cands * args.steps / (a.elapsed_time(b) / 1e3)
+        same_cps = n_cands * steps / (a.elapsed_time(b) / 1e3)
         for wd in words:
             mg.set_shape_override(mg.PATH_BATCHED, wd, -1)
     ctx.close()
     del d_peq, d_qi, d_c, d_res
+    torch.cuda.empty_cache()
 
-    rates = [1e4, 1e5, 1e6, 2e6, 5e6, 1e7, 2e7, 3e7, 4e7, 5e7, 6e7, 7e7, 7.5e7, 8e7, 8.2e7, 8.4e7, 8.6e7, 8.8e7,
-             9e7, 9.2e7, 9.5e7, 1e8,
-             1.1e8]
     rng = np.random.default_rng(5)
     sweep, same = [], True
     clocks = ClockSampler(0)
@@ -622,30 +811,57 @@ def run_serving(args):
                           "throughput_cand_s": cands_done / (wall / 1e9),
                           "p50_ms": float(np.percentile(lat[ok], 50) / 1e6), "p99_ms": float(np.percentile(lat[ok], 99) / 1e6),
                           "status": int(stt)})
+            clocks.poke()
         stats = srv.stats()
     clk = clocks.stop()
-    ref.close()
     good = [r for r in sweep if r["p99_ms"] <= 5.0 and r["refused"] == 0]
     best = max(good, key=lambda r: r["throughput_cand_s"]) if good else None
     value = best["throughput_cand_s"] if best else 0.0
+    rec = {"workload": WORKLOAD_NAMES[5], "requests": n_req, "candidates": n_cands,
+           "served_cand_s_at_p99_le_5ms": value, "best": best, "batched_cand_s": batched_cps,
+           "served_frac_of_batched": value / batched_cps, "batched_same_shapes_cand_s": same_cps,
+           "served_frac_of_batched_same_shapes": (value / same_cps) if same_cps else None,
+           "results_equal_to_batched": same, "batches": stats["batches"],
+           "largest_batch_candidates": stats["batchCandidatesMax"],
+           "server": {"slots": stats["slots"], "max_batch_candidates": stats["maxBatchCandidates"],
+                      "budget": "16 GiB", "lane_words": args.lane_words, "graphs": not args.no_graphs},
+           "sweep": sweep, "clocks": clk}
+    if threads:
+        rec["parity_sample"], rec["cpu_baseline"] = reference_parity(w, batched_res, ref_words, ref_size,
+                                                                     args.parity_frac, 505, threads, padded)
+    return rec
+
+
+def run_serving(args):
+    """Workload 5 alone: the full offered-rate sweep."""
+    import torch
+
+    import myersgpu as mg
+    import myerssynth as ms
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    torch.cuda.set_device(0)
+    ref_words, ref_size = reference_words(ms, 5)
+    ref = mg.Reference(ref_words, ref_size)
+    try:
+        rec = serving_sweep(mg, ms, args, ref, ref_words, ref_size, SERVING_RATES_FULL, args.steps, args.warmup,
+                            0 if args.no_cpu else host_threads())
+    finally:
+        ref.close()
+    value = rec["served_cand_s_at_p99_le_5ms"]
     line = {"metric": "candidates/s served at p99 <= 5 ms", "value": value, "unit": "candidates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded), open-loop Poisson arrivals",
-            "config": {"workload": WORKLOAD_NAMES[5], "requests": n_req, "candidates": n_cands, "distance": DIST,
-                       "server": {"slots": stats["slots"], "max_batch_candidates": stats["maxBatchCandidates"],
-                                  "budget": "16 GiB", "lane_words": args.lane_words,
-                                  "graphs": not args.no_graphs}},
-            "serving": {"sweep": sweep, "best": best, "batched_cand_s": batched_cps,
-                        "served_frac_of_batched": value / batched_cps,
-                        "batched_same_shapes_cand_s": same_cps,
-                        "served_frac_of_batched_same_shapes": (value / same_cps) if same_cps else None,
-                        "results_equal_to_batched": same, "batches": stats["batches"],
-                        "largest_batch_candidates": stats["batchCandidatesMax"]},
+            "config": {"workload": WORKLOAD_NAMES[5], "requests": rec["requests"], "candidates": rec["candidates"],
+                       "distance": DIST, "server": rec["server"]},
+            "serving": {k: v for k, v in rec.items() if k not in ("clocks", "server", "workload")},
             "e2e": {"value": value, "unit": "candidates/s",
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "api": "myersServerSubmit/Wait through the replay driver: arrival to results on the host"},
-            "clocks": clk, "gpu_launches": None}
+            "clocks": rec["clocks"], "gpu_launches": None}
     print(json.dumps(line), flush=True)
 
 
@@ -656,9 +872,10 @@ def run_traceback(args):
     import torch
 
     import myersgpu as mg
+    import myerssynth as ms
     torch.cuda.set_device(0)
     k = args.workload
-    s, ref_words, ref_size, w = make_inputs(mg, k, args.scale, 0)
+    s, ref_words, ref_size, w = make_inputs(ms, k, args.scale, 0)
     n = len(w["cands"])
     m_of = w["qinfo"]["size"][w["cands"]["query"]].astype(np.int64)
     max_score = int(args.tb_bound * int(m_of.max()))
@@ -738,8 +955,7 @@ def run_traceback(args):
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
         "config": {"workload": "traceback of " + WORKLOAD_NAMES[k], "traced": int(traced), "candidates": n,
-                   "max_score": max_score, "max_ops": max_ops, "scratch_gib": args.tb_scratch_gb,
-                   "l2": "L2 flushed before every timed step (256 MiB write, untimed)"},
+                   "max_score": max_score, "max_ops": max_ops, "scratch_gib": args.tb_scratch_gb, "l2": L2_NOTE},
         "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
                      "frac": achieved / peak, "traffic": None,
                      "note": "whole call (selection, host read of the count, forward pass, walk) against the "

@@ -163,6 +163,13 @@ int myersSetKernelPath(void *myersBuffer, int path);
 /* Non-zero (default): replay each send as a CUDA graph; 0: plain stream
  * launches. The environment variable MYERS_GRAPHS=0 sets the default to 0. */
 int myersSetGraphs(void *myersBuffer, int enable);
+/* Ukkonen's cut-off for the buffer's sends (see myersVerifyCutoffAsync):
+ * cutoff >= 0 reports a candidate whose minimum exceeds (uint32_t)(m *
+ * cutoff) as {MYERS_NO_MATCH, MYERS_NO_MATCH}; cutoff < 0 (default) turns it
+ * off. Replaces gt_map_block_bpm_get_distance__cutoff
+ * (GEMTools/src/gt_map_align_bpm.c:141-210) for a verifier whose caller
+ * drops candidates above an error bound anyway. */
+int myersSetCutoff(void *myersBuffer, float cutoff);
 
 /* Device memory budget (bytes) for all buffers created by the next
  * initMyers/myersInit, replacing the reference's "95% of free memory"
@@ -224,15 +231,40 @@ int myersVerifyRangeAsync(myersContext_t *ctx, const myersReference_t *ref,
                           uint32_t minQuerySize, uint32_t maxQuerySize,
                           resEntry_t *d_results, void *stream);
 
+/* Column and score of a candidate whose minimum exceeds the cut-off bound. */
+#define MYERS_NO_MATCH 0xFFFFFFFFu
+
+/* As myersVerifyRangeAsync, under Ukkonen's cut-off with the bound
+ * k = (uint32_t)(m * cutoff) (float32) for a query of m bases. The analogue of
+ * GEMTools' gt_map_block_bpm_get_distance__cutoff
+ * (GEMTools/src/gt_map_align_bpm.c:141-210), which returns the distance and
+ * position only when the minimum is within its max_distance:
+ *  - a candidate whose minimum score is <= k gets exactly the result of
+ *    myersVerifyRangeAsync (score, first column of that score);
+ *  - a candidate whose minimum exceeds k gets {MYERS_NO_MATCH, MYERS_NO_MATCH};
+ *  - candidates that are not verified (window out of range, invalid indices,
+ *    unsupported sizes) get {0, 0xFFFFFFFF} as without the cut-off.
+ * On the plain path, queries of 225..1024 bases whose bucket runs one
+ * candidate per lane with a multiple of 4 words skip the DP rows that cannot
+ * reach k (rows are skipped 128 at a time, per warp); every other shape, and
+ * the batched path, compute every row and apply the same contract. */
+int myersVerifyCutoffAsync(myersContext_t *ctx, const myersReference_t *ref,
+                           const qryEntry_t *d_peq, uint32_t numPEQEntries,
+                           const qryInfo_t *d_qinfo, uint32_t numQueries,
+                           const candInfo_t *d_cands, uint32_t numCandidates,
+                           float distance, int windowMode, int path, float cutoff,
+                           uint32_t minQuerySize, uint32_t maxQuerySize,
+                           resEntry_t *d_results, void *stream);
+
 /* Largest batch myersVerifyNoAllocAsync accepts (candidates). */
 #define MYERS_NOALLOC_MAX_CANDIDATES 262144u
 
 /* Verification that allocates nothing. No counterpart in the reference.
  *
- * For callers that cannot call cudaMalloc: code that runs while a stream is
- * being captured into a CUDA graph, programs whose allocator owns all of
- * device memory (a caching allocator or an arena carved out at start-up), and
- * services whose memory budget is frozen once they are up. Inputs and outputs
+ * For callers that cannot call cudaMalloc: programs whose own allocator owns
+ * all of device memory (a caching allocator, or an arena carved out at
+ * start-up, where an outside cudaMalloc fails or fragments the pool), and
+ * services whose memory budget is fixed once they are up. Inputs and outputs
  * are the caller's device memory, as for myersVerifyRangeAsync, and the
  * reference is passed as raw device words (refWords readable words holding
  * refSizeBases bases; reads past them act as N). It runs the batched path;
@@ -241,8 +273,11 @@ int myersVerifyRangeAsync(myersContext_t *ctx, const myersReference_t *ref,
  *
  *  - at most MYERS_NOALLOC_MAX_CANDIDATES candidates per call; larger batches
  *    return MYERS_E_CAPACITY and enqueue nothing;
- *  - the first call on a device resolves the array's device address (with
- *    that device current); make that first call before any stream capture;
+ *  - the first call on a device (and again after that device's context was
+ *    reset) does the set-up, with that device current: it looks up the
+ *    array's device address and loads every kernel this entry point can
+ *    launch, so later calls load no code; make that first call before any
+ *    stream capture;
  *  - every call on a device shares the one array and leaves its contents
  *    behind (each call clears what must start at zero): calls that overlap on
  *    the GPU (other streams, or other threads) race and give wrong results;

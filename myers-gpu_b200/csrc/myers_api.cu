@@ -24,6 +24,7 @@
 #include <vector>
 
 #include <dlfcn.h>
+#include <cuda.h>  // driver types only: entry points come through cudaGetDriverEntryPointByVersion
 #include <cuda_runtime.h>
 
 #include "../../include/myers-interface.h"
@@ -125,12 +126,19 @@ extern "C" int myersReferenceCreate(myersReference_t** ref, const uint32_t* host
 
 // File format of src-api/genReference-4bits.c:121-140: u32 numEntries,
 // u32 size, then numEntries packed words (read at src-api/myersGPU.c:106-128).
+// The header is checked against the file's length before anything is
+// allocated: a file that is shorter than its header says, or whose base count
+// exceeds its words, is MYERS_E_READING_FILE (the reference reads whatever
+// fread returns, myersGPU.c:117-122).
 extern "C" int myersReferenceLoad(myersReference_t** ref, const char* fileName) {
   if (ref == nullptr || fileName == nullptr) return MYERS_E_INVALID_ARGUMENT;
   FILE* fp = fopen(fileName, "rb");
   if (fp == nullptr) return MYERS_E_OPENING_FILE;
   uint32_t hdr[2];
-  if (fread(hdr, sizeof(uint32_t), 2, fp) != 2) {
+  long long file_bytes = -1;
+  if (fseek(fp, 0, SEEK_END) == 0) file_bytes = ftell(fp);
+  if (file_bytes < 8 || fseek(fp, 0, SEEK_SET) != 0 || fread(hdr, sizeof(uint32_t), 2, fp) != 2 ||
+      (unsigned long long)file_bytes < 8ull + 4ull * hdr[0] || (uint64_t)hdr[1] > (uint64_t)hdr[0] * 8) {
     fclose(fp);
     return MYERS_E_READING_FILE;
   }
@@ -423,11 +431,18 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     // no query needs the DP (all empty or all too long): classify alone
     // writes every result
   }
+  // a plain launch of shape c: under the cut-off, the single-lane shapes
+  // that have a cut-off kernel skip the rows above the band
+  auto plain = [&](uint32_t c, const uint32_t* ids, const BucketState* st, uint32_t count, uint32_t* next) {
+    const Shape sh = plan.shape[c];
+    if (in.cut && has_cutoff_kernel(sh.variant))
+      return launch_cutoff(sh.variant, in, ids, st, (int)c, 0, count, next, s, ctx->num_sms);
+    return launch_plain(sh.variant, sh.L, in, ids, st, (int)c, 0, count, next, s, ctx->num_sms);
+  };
   if (path == MYERS_PATH_PLAIN && plan.num_cfg == 1) {
-    const Shape sh = plan.shape[0];
     uint32_t* next = &ctx->d_state->next[0];  // the launch's tile counter
     CU(cudaMemsetAsync(next, 0, sizeof(uint32_t), s));
-    CU(launch_plain(sh.variant, sh.L, in, nullptr, nullptr, 0, 0, in.num_cands, next, s, ctx->num_sms));
+    CU(plain(0, nullptr, nullptr, in.num_cands, next));
     ctx->last_launches = 1;
     return MYERS_SUCCESS;
   }
@@ -442,8 +457,7 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     first_plain = plan.num_batched;
   }
   for (uint32_t c = first_plain; c < plan.num_cfg; ++c) {
-    CU(launch_plain(plan.shape[c].variant, plan.shape[c].L, in, ctx->d_ids, ctx->d_state, (int)c, 0, 0,
-                    &ctx->d_state->next[c], s, ctx->num_sms));
+    CU(plain(c, ctx->d_ids, ctx->d_state, 0, &ctx->d_state->next[c]));
     ++launches;
   }
   ctx->last_launches = launches;
@@ -468,11 +482,42 @@ extern "C" int myersVerifyAsync(myersContext_t* ctx, const myersReference_t* ref
                                distance, windowMode, path, 0, 0, d_results, stream);
 }
 
+static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
+                        uint32_t numPEQEntries, const qryInfo_t* d_qinfo, uint32_t numQueries,
+                        const candInfo_t* d_cands, uint32_t numCandidates, float distance, int windowMode, int path,
+                        float cutoff, uint32_t minQuerySize, uint32_t maxQuerySize, resEntry_t* d_results,
+                        void* stream);
+
 extern "C" int myersVerifyRangeAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
                                      uint32_t numPEQEntries, const qryInfo_t* d_qinfo, uint32_t numQueries,
                                      const candInfo_t* d_cands, uint32_t numCandidates, float distance,
                                      int windowMode, int path, uint32_t minQuerySize, uint32_t maxQuerySize,
                                      resEntry_t* d_results, void* stream) {
+  return verify_range(ctx, ref, d_peq, numPEQEntries, d_qinfo, numQueries, d_cands, numCandidates, distance,
+                      windowMode, path, -1.0f, minQuerySize, maxQuerySize, d_results, stream);
+}
+
+// Ukkonen's cut-off (GEMTools/src/gt_map_align_bpm.c:141-210,
+// gt_map_block_bpm_get_distance__cutoff): the result is exact where the
+// minimum is at most (uint32_t)(m * cutoff), else {MYERS_NO_MATCH,
+// MYERS_NO_MATCH}. The plain path's single-lane shapes of 8..32 words (a
+// multiple of 4) skip the rows above the band; other shapes and the batched
+// path compute every row and apply the same contract.
+extern "C" int myersVerifyCutoffAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
+                                      uint32_t numPEQEntries, const qryInfo_t* d_qinfo, uint32_t numQueries,
+                                      const candInfo_t* d_cands, uint32_t numCandidates, float distance,
+                                      int windowMode, int path, float cutoff, uint32_t minQuerySize,
+                                      uint32_t maxQuerySize, resEntry_t* d_results, void* stream) {
+  if (!(cutoff >= 0.0f) || !std::isfinite(cutoff)) return MYERS_E_INVALID_ARGUMENT;
+  return verify_range(ctx, ref, d_peq, numPEQEntries, d_qinfo, numQueries, d_cands, numCandidates, distance,
+                      windowMode, path, cutoff, minQuerySize, maxQuerySize, d_results, stream);
+}
+
+static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
+                        uint32_t numPEQEntries, const qryInfo_t* d_qinfo, uint32_t numQueries,
+                        const candInfo_t* d_cands, uint32_t numCandidates, float distance, int windowMode, int path,
+                        float cutoff, uint32_t minQuerySize, uint32_t maxQuerySize, resEntry_t* d_results,
+                        void* stream) {
   if (ctx == nullptr || ref == nullptr) return MYERS_E_INVALID_ARGUMENT;
   if (!(distance >= 0.0f) || !std::isfinite(distance)) return MYERS_E_INVALID_ARGUMENT;
   if (windowMode != MYERS_WINDOW_ALIGNED && windowMode != MYERS_WINDOW_EXACT) return MYERS_E_INVALID_ARGUMENT;
@@ -493,6 +538,8 @@ extern "C" int myersVerifyRangeAsync(myersContext_t* ctx, const myersReference_t
   in.num_entries = numPEQEntries;
   in.distance = distance;
   in.exact = windowMode == MYERS_WINDOW_EXACT;
+  in.cut = cutoff >= 0.0f;
+  in.cutoff = in.cut ? cutoff : 0.0f;
   return verify_enqueue(ctx, ref, in, plan, path, (cudaStream_t)stream);
 }
 
@@ -658,6 +705,7 @@ struct Buffer {
   resEntry_t* d_results;
   int window_mode;
   int path;
+  float cutoff;  // < 0: off
   int use_graphs;
   cudaGraphExec_t exec;  // the last send, updated in place by the next
   int last_status;
@@ -730,7 +778,12 @@ extern "C" int myersInit(void*** myersBuffer, uint32_t numBuffers, const char* r
   if (st != MYERS_SUCCESS) return st;
   Shared* shared = new Shared{ref, 0};
   size_t freeb = 0, totalb = 0;
-  CU(cudaMemGetInfo(&freeb, &totalb));
+  const cudaError_t me = cudaMemGetInfo(&freeb, &totalb);
+  if (me != cudaSuccess) {
+    myersReferenceDestroy(ref);
+    delete shared;
+    return cuda_fail(me, "cudaMemGetInfo");
+  }
   // sizing as src-api/myersGPU.c:312-330, over the budget instead of free memory
   const uint32_t entries_per_query = (averageQuerySize + NUM_BASES_ENTRY - 1) / NUM_BASES_ENTRY;
   const double bytes_per_cand = (entries_per_query * sizeof(qryEntry_t) + sizeof(qryInfo_t)) / (double)candidatesPerQuery +
@@ -746,7 +799,11 @@ extern "C" int myersInit(void*** myersBuffer, uint32_t numBuffers, const char* r
     return MYERS_E_INSUFFICIENT_MEM_GPU;
   }
   Buffer** bufs = (Buffer**)calloc(numBuffers, sizeof(Buffer*));
-  if (bufs == nullptr) return MYERS_E_ALLOCATE_MEM;
+  if (bufs == nullptr) {
+    myersReferenceDestroy(ref);
+    delete shared;
+    return MYERS_E_ALLOCATE_MEM;
+  }
   for (uint32_t i = 0; i < numBuffers; ++i) {
     Buffer* b = new Buffer();
     b->numBuffers = numBuffers;
@@ -759,6 +816,7 @@ extern "C" int myersInit(void*** myersBuffer, uint32_t numBuffers, const char* r
     shared->refs++;
     b->window_mode = MYERS_WINDOW_ALIGNED;
     b->path = MYERS_PATH_PLAIN;
+    b->cutoff = -1.0f;
     const char* p = getenv("MYERS_PATH");
     if (p && strcmp(p, "batched") == 0) b->path = MYERS_PATH_BATCHED;
     const char* g = getenv("MYERS_GRAPHS");
@@ -825,6 +883,8 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
     in.num_entries = numPEQEntries;
     in.distance = distance;
     in.exact = b->window_mode == MYERS_WINDOW_EXACT;
+    in.cut = b->cutoff >= 0.0f;
+    in.cutoff = in.cut ? b->cutoff : 0.0f;
     const int est = verify_enqueue(b->ctx, b->shared->ref, in, plan, b->path, s);
     if (est != MYERS_SUCCESS) return est;
     CU(cudaMemcpyAsync(b->h_results, b->d_results, (size_t)numCandidates * sizeof(resEntry_t),
@@ -883,6 +943,13 @@ extern "C" int myersSetKernelPath(void* mb, int path) {
   return MYERS_SUCCESS;
 }
 
+extern "C" int myersSetCutoff(void* mb, float cutoff) {
+  Buffer* b = static_cast<Buffer*>(mb);
+  if (b == nullptr || std::isnan(cutoff) || std::isinf(cutoff)) return MYERS_E_INVALID_ARGUMENT;
+  b->cutoff = cutoff < 0.0f ? -1.0f : cutoff;
+  return MYERS_SUCCESS;
+}
+
 extern "C" int myersSetGraphs(void* mb, int enable) {
   Buffer* b = static_cast<Buffer*>(mb);
   if (b == nullptr) return MYERS_E_INVALID_ARGUMENT;
@@ -899,10 +966,10 @@ extern "C" uint32_t myersBufferLastLaunches(void* mb) {
 // ---------------------------------------------------------------------------
 // Verification that allocates nothing (no counterpart in the reference).
 //
-// Some callers cannot call cudaMalloc: code running while a stream is being
-// captured into a CUDA graph, allocators that own all of device memory
-// (a caching allocator or a fixed arena handed out once), and services whose
-// memory budget is frozen after start-up. For them this entry point runs the
+// Some callers cannot call cudaMalloc: programs whose own allocator owns all
+// of device memory (a caching allocator, or a fixed arena handed out once,
+// where an outside cudaMalloc fails or fragments it), and services whose
+// memory budget is fixed after start-up. For them this entry point runs the
 // batched path with its bucketing scratch (candidate ids sorted by shape, a
 // shape byte per candidate, the bucket table and the error flags) in the
 // file-scope device array below instead of a context's allocations. The
@@ -923,30 +990,65 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocDevice {
   bool ready;
-  unsigned char* scratch;  // device address of g_noalloc_scratch on this device
+  unsigned long long context;  // id of the context the set-up ran in (0: unknown)
+  unsigned char* scratch;      // device address of g_noalloc_scratch in that context
   int num_sms;
 };
 static std::mutex g_noalloc_mu;
 static NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 
-// Once per device, with that device current: resolve the array's device
-// address (this may load the module, so it should not happen inside a
-// stream capture; the first call on each device does it).
+// Id of the current CUDA context, unique for the life of the process (0 if
+// no context is current or the driver cannot tell). Driver entry points are
+// looked up through the runtime, so the library needs no link to libcuda.
+static unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&get_current, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&get_id, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current == nullptr || get_id == nullptr || get_current(&c) != CUDA_SUCCESS || c == nullptr ||
+      get_id(c, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
+
+// Once per device, with that device current (and again when the device's
+// context is not the one the set-up ran in, e.g. after cudaDeviceReset):
+// resolve the array's device address and load every kernel this entry point
+// can launch. Both may load code onto the device, so the first call should
+// come before any stream capture.
 static int noalloc_setup(NoAllocDevice* out) {
   int dev = 0;
   CU(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices) return MYERS_E_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   NoAllocDevice& d = g_noalloc_dev[dev];
-  if (!d.ready) {
+  const unsigned long long ctx = current_context_id();
+  if (!d.ready || (ctx != 0 && ctx != d.context)) {
+    d.ready = false;
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
+    e = load_batched_path_kernels();
+    if (e != cudaSuccess) return cuda_fail(e, "loading the batched path's kernels");
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
     d.scratch = static_cast<unsigned char*>(p);
     d.num_sms = sms;
+    d.context = current_context_id();  // the set-up made the primary context current if none was
     d.ready = true;
   }
   *out = d;
@@ -961,7 +1063,7 @@ extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refW
                                        resEntry_t* d_results, void* stream) {
   if (!(distance >= 0.0f) || !std::isfinite(distance)) return MYERS_E_INVALID_ARGUMENT;
   if (windowMode != MYERS_WINDOW_ALIGNED && windowMode != MYERS_WINDOW_EXACT) return MYERS_E_INVALID_ARGUMENT;
-  if (refSizeBases > refWords * 8) return MYERS_E_INVALID_ARGUMENT;
+  if (refWords > UINT64_MAX / 8 || refSizeBases > refWords * 8) return MYERS_E_INVALID_ARGUMENT;
   if (numCandidates > kNoAllocMax) return MYERS_E_CAPACITY;  // beyond the static scratch
   if (numCandidates == 0) return MYERS_SUCCESS;
   if (d_refWords == nullptr || d_peq == nullptr || d_qinfo == nullptr || d_cands == nullptr || d_results == nullptr)

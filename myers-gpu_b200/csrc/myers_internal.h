@@ -12,6 +12,8 @@ constexpr uint32_t kPadWord = 0x44444444u;
 // window reads past the last packed word stay inside the allocation.
 constexpr uint64_t kRefPadWords = 64;
 constexpr uint32_t kNoResult = 0xFFFFFFFFu;
+// Column and score of a candidate whose minimum exceeds the cut-off bound.
+constexpr uint32_t kNoMatch = 0xFFFFFFFFu;
 constexpr uint32_t kMaxWords = 1024;          // 32768 bases
 constexpr uint32_t kMaxColumns = 65535;       // the result key keeps 16 column bits
 
@@ -90,9 +92,13 @@ struct DevInputs {
   uint32_t num_entries;
   float distance;
   int exact;
+  // Ukkonen cut-off: with `cut` set, a candidate whose minimum score exceeds
+  // (uint32_t)(m * cutoff) (float32) gets {kNoMatch, kNoMatch}.
+  float cutoff;
+  int cut;
   // Multipliers the compiler cannot fold (set by set_multipliers): they keep
   // the per-column bookkeeping on the FMA pipe (see myers_kernels.cu).
-  uint32_t one, two, k16, mk16, p28, kb33, kb17, mn16;
+  uint32_t one, two, k16, mk16, p28, kb33, kb17, mn16, mone;
 };
 
 inline void set_multipliers(DevInputs& in) {
@@ -104,6 +110,7 @@ inline void set_multipliers(DevInputs& in) {
   in.kb33 = 33u * 4u * 4u;  // bytes between the bases of a PEQ group, 33 columns
   in.kb17 = 17u * 4u * 4u;  // ... 17 columns
   in.mn16 = 0xFFFFFFF0u;    // -16
+  in.mone = 0xFFFFFFFFu;    // -1
 }
 
 inline int variant_W(int v) { return v < kNumSingle ? v + 1 : kMultiW[v - kNumSingle]; }
@@ -123,12 +130,25 @@ int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_
 cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
                          int cfg, uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms);
 
+// Whether the plain path has a cut-off kernel for variant v (single-lane
+// shapes of 8..32 words, a multiple of 4), and one launch of it; arguments
+// as launch_plain.
+bool has_cutoff_kernel(int v);
+cudaError_t launch_cutoff(int v, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state, int cfg,
+                          uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms);
+
 // The persistent batched launch over the plan's first num_batched shapes;
 // the grid is the device's resident capacity or, for small batches, one
 // warp per tile of `max_tiles` (an upper bound of the tiles), whichever is
 // smaller, so concurrent small batches share the device.
 cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,
                            BucketState* d_state, cudaStream_t s, int num_sms, uint32_t max_tiles);
+
+// Load every kernel the batched path can launch (bucketing, the persistent
+// kernel, the plain launches of shapes it does not carry) on the current
+// device. With lazy module loading a kernel is otherwise loaded, and its code
+// allocated on the device, at its first launch.
+cudaError_t load_batched_path_kernels();
 
 // Bytes of shared memory one warp needs for a shape.
 uint32_t warp_smem_bytes(int v, int L);

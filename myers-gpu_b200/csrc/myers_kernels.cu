@@ -124,10 +124,11 @@ struct Mul {
   uint32_t p28;        // 1 << 28: umulhi(x, p28) = x >> 4
   uint32_t kb33, kb17; // bytes between bases of a group for 33 / 17 columns
   uint32_t mn16;       // -16
+  uint32_t mone;       // -1
 };
 
 __device__ __forceinline__ Mul make_mul(const DevInputs& in) {
-  return Mul{in.one, in.two, in.k16, in.mk16, in.p28, in.kb33, in.kb17, in.mn16};
+  return Mul{in.one, in.two, in.k16, in.mk16, in.p28, in.kb33, in.kb17, in.mn16, in.mone};
 }
 
 #ifndef MYERS_FMA_KEY
@@ -177,17 +178,42 @@ __device__ __forceinline__ uint32_t base_bytes(Mul k) {
   return Layout<W, MULTI>::NCOL == 33 ? k.kb33 : k.kb17;
 }
 
+// How the words of the multi-word add are formed: 0 add/addc (ALU pipe);
+// 1 every word as a multiply-add by an opaque one with carry (mad.lo.cc /
+// madc.lo.cc); 2 the odd words that way.
+#ifndef MYERS_MADC_ADD
+#define MYERS_MADC_ADD 0
+#endif
+
 // s = a + b over W words with the carry rippling through the CC flag.
 template <int W>
-__device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t (&b)[W], uint32_t (&s)[W]) {
+__device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t (&b)[W], uint32_t (&s)[W],
+                                          uint32_t one) {
   if constexpr (W == 1) {
+    (void)one;
     s[0] = a[0] + b[0];
-  } else {
+  } else if constexpr (MYERS_MADC_ADD == 0) {
+    (void)one;
     asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(a[0]), "r"(b[0]));
 #pragma unroll
     for (int j = 1; j < W - 1; ++j)
       asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s[j]) : "r"(a[j]), "r"(b[j]));
     asm volatile("addc.u32 %0, %1, %2;" : "=r"(s[W - 1]) : "r"(a[W - 1]), "r"(b[W - 1]));
+  } else {
+    constexpr int ALL = MYERS_MADC_ADD == 1;
+    if (ALL) asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(s[0]) : "r"(a[0]), "r"(one), "r"(b[0]));
+    else asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(a[0]), "r"(b[0]));
+#pragma unroll
+    for (int j = 1; j < W - 1; ++j) {
+      if (ALL || (j & 1))
+        asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(s[j]) : "r"(a[j]), "r"(one), "r"(b[j]));
+      else
+        asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s[j]) : "r"(a[j]), "r"(b[j]));
+    }
+    if (ALL || ((W - 1) & 1))
+      asm volatile("madc.lo.u32 %0, %1, %2, %3;" : "=r"(s[W - 1]) : "r"(a[W - 1]), "r"(one), "r"(b[W - 1]));
+    else
+      asm volatile("addc.u32 %0, %1, %2;" : "=r"(s[W - 1]) : "r"(a[W - 1]), "r"(b[W - 1]));
   }
 }
 
@@ -205,34 +231,49 @@ __device__ __forceinline__ void add_chain(const uint32_t (&a)[W], const uint32_t
 #define MYERS_FMA_SHIFT_MULTI 0
 #endif
 
-// FMA-pipe shifts for shape (W, MULTI) in the plain or the persistent kernel.
+// Which of a column's one-bit shifts run on the FMA pipe (a shift policy):
+//   0  none (funnel shifts on the ALU pipe)
+//   1  all of them
+//   2  the Ph shifts of every word, the Mh shifts on the ALU pipe
+//   3  both shifts of the odd words
+//   4  the Ph shifts of the odd words
+// Single-lane shapes of more than MYERS_FMA_SHIFT_MAX_W words use policy
+// MYERS_FMA_SHIFT_WIDE.
+#ifndef MYERS_FMA_SHIFT_WIDE
+#define MYERS_FMA_SHIFT_WIDE 0
+#endif
+
+// The shift policy of shape (W, MULTI) in the plain or the persistent kernel.
 template <int W, bool MULTI, bool PERSISTENT>
-__host__ __device__ constexpr bool fma_shift() {
-  return W <= MYERS_FMA_SHIFT_MAX_W && (!MULTI || MYERS_FMA_SHIFT_MULTI) &&
-         (!PERSISTENT || MYERS_FMA_SHIFT_BATCHED);
+__host__ __device__ constexpr int fma_shift() {
+  if (MYERS_SHIFT_MODE == 2) return 1;
+  if (PERSISTENT && !MYERS_FMA_SHIFT_BATCHED) return 0;
+  if (MULTI) return MYERS_FMA_SHIFT_MULTI ? 1 : 0;
+  return W <= MYERS_FMA_SHIFT_MAX_W ? 1 : MYERS_FMA_SHIFT_WIDE;
+}
+
+// Whether the Ph (ph = true) or Mh shift of word j runs on the FMA pipe
+// under policy FS. j is a constant after unrolling, so this folds away.
+template <int FS>
+__device__ __forceinline__ bool fma_word(int j, bool ph) {
+  return FS == 1 || (FS == 2 && ph) || (FS == 3 && (j & 1)) || (FS == 4 && ph && (j & 1));
 }
 
 // (cur << 1) | (prev >> 31): the one-bit shift of a multi-word vector.
 // On the ALU pipe: one funnel shift. On the FMA pipe: multiply-high and
 // multiply-add by an opaque two -- fewer ALU instructions but more
 // instructions and latency in all, which only pays where many warps are
-// resident (narrow shapes). FMA for shapes of at most MYERS_FMA_SHIFT_MAX_W
-// words (MYERS_SHIFT_MODE=2: all shapes).
-template <bool FS>
-__device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k) {
-  if constexpr (MYERS_SHIFT_MODE == 2 || FS) {
-    return cur * k.two + __umulhi(prev, k.two);
-  } else {
-    (void)k;
-    return __funnelshift_l(prev, cur, 1);
-  }
+// resident (narrow shapes).
+__device__ __forceinline__ uint32_t shl1(uint32_t prev, uint32_t cur, Mul k, bool fma) {
+  if (fma) return cur * k.two + __umulhi(prev, k.two);
+  return __funnelshift_l(prev, cur, 1);
 }
 
 // One text column over W words. With HIN, bit 31 of inP / inM is the
 // horizontal delta (+1 / -1) entering the bottom row (Myers' block rule);
 // without, it is 0 (semi-global: row 0 of the DP is all zeros).
 // topP / topM return the unshifted top words (bit 31 = delta out of the top row).
-template <int W, bool HIN, bool FS>
+template <int W, bool HIN, int FS>
 __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (&Pv)[W], uint32_t (&Mv)[W],
                                              uint32_t inP, uint32_t inM, uint32_t& topP, uint32_t& topM, Mul k) {
   uint32_t e0 = eq[0];
@@ -241,7 +282,7 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
   t[0] = e0 & Pv[0];
 #pragma unroll
   for (int j = 1; j < W; ++j) t[j] = eq[j] & Pv[j];
-  add_chain<W>(t, Pv, s);
+  add_chain<W>(t, Pv, s, k.one);
   uint32_t php = HIN ? inP : 0u, mhp = HIN ? inM : 0u;
 #pragma unroll
   for (int j = 0; j < W; ++j) {
@@ -251,8 +292,8 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
     const uint32_t xh = (s[j] ^ pv) | e;
     const uint32_t ph = mv | ~(xh | pv);
     const uint32_t mh = pv & xh;
-    const uint32_t phs = shl1<FS>(php, ph, k);
-    const uint32_t mhs = shl1<FS>(mhp, mh, k);
+    const uint32_t phs = shl1(php, ph, k, fma_word<FS>(j, true));
+    const uint32_t mhs = shl1(mhp, mh, k, fma_word<FS>(j, false));
     Pv[j] = mhs | ~(xv | phs);
     Mv[j] = phs & xv;
     php = ph;
@@ -265,7 +306,7 @@ __device__ __forceinline__ void myers_column(const uint32_t (&eq)[W], uint32_t (
 // Eight columns of one text word, single-lane shapes. TAIL masks columns >= n.
 // Eight columns of one text word (codes 0..4 in its nibbles), single-lane
 // shapes. TAIL masks columns >= n.
-template <int W, bool TAIL, int UNR, bool FS>
+template <int W, bool TAIL, int UNR, int FS>
 __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                               uint32_t (&Mv)[W], uint32_t& sc, uint32_t& kmin,
                                               uint32_t colbase, uint32_t n, Mul k) {
@@ -292,7 +333,7 @@ __device__ __forceinline__ void block8_single(uint32_t t, const char* __restrict
 // outside their candidate's columns (pipeline fill and drain, shorter
 // candidates); otherwise every lane with work is inside (steady state), and
 // lanes without work compute values nobody reads.
-template <int W, bool CHECKED, int UNR, bool FS>
+template <int W, bool CHECKED, int UNR, int FS>
 __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
                                              uint32_t (&Mv)[W], uint32_t& outP, uint32_t& outM, uint32_t& sc,
                                              uint32_t& kmin, uint32_t jbase, uint32_t n, bool work,
@@ -325,6 +366,27 @@ __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict_
 #endif
   }
 }
+
+// The cut-off bound of a query of m bases: (uint32_t)(m * cutoff) in float32.
+__device__ __forceinline__ uint32_t d_cutoff_bound(uint32_t m, float cutoff) {
+  return (uint32_t)__fmul_rn((float)m, cutoff);
+}
+
+// The result of a verified candidate from its (score << 16 | column) key,
+// whose score carries the p padding rows. Under the cut-off contract a
+// minimum above the bound is reported as {kNoMatch, kNoMatch}.
+__device__ __forceinline__ uint2 result_of(const DevInputs& in, uint32_t kmin, uint32_t p, uint32_t m) {
+  const uint32_t score = (kmin >> 16) - p;
+  if (in.cut && score > d_cutoff_bound(m, in.cutoff)) return make_uint2(kNoMatch, kNoMatch);
+  return make_uint2(kmin & 0xFFFFu, score);
+}
+
+// Multi-lane shapes: run the pipeline's ramp-up, steady state and drain as
+// three loops instead of one loop that picks the checked or unchecked step
+// per block of 8 columns.
+#ifndef MYERS_MULTI_SPLIT
+#define MYERS_MULTI_SPLIT 0
+#endif
 
 struct CandSetup {
   uint32_t id;
@@ -391,7 +453,7 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
 // UNR: how far the 8 columns of a text word are unrolled -- fully for the
 // one-shape plain kernels; partly in the persistent kernel, whose code holds
 // every shape and would otherwise overflow the instruction cache.
-template <int W, bool MULTI, int UNR = 8, bool FS = false>
+template <int W, bool MULTI, int UNR = 8, int FS = 0>
 __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
                                              uint32_t cnt, int L, uint32_t* __restrict__ wsmem, int lane) {
   using Lay = Layout<W, MULTI>;
@@ -462,7 +524,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
           const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
           block8_single<W, true, UNR, FS>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
         }
-        in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
+        in.results[c.id] = result_of(in, kmin, p, c.m);
       }
     } else {
       uint32_t steps = work ? c.n + (uint32_t)L - 1u : 0u;
@@ -474,6 +536,35 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
       uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
       uint32_t outP = 0u, outM = 0u;
       const uint32_t segmul = (uint32_t)min(l, 1);
+#if MYERS_MULTI_SPLIT
+      // blocks [i_lo, i_hi) have every lane with work inside its columns:
+      // 8i + 1 >= L and 8i + 8 <= n_min. The ramp-up, the steady state and the
+      // drain run as separate loops, so no block tests which one it is in.
+      const uint32_t i_lo = min(((uint32_t)L + 6u) >> 3, nblk);
+      const uint32_t i_hi = max(min(n_min >> 3, nblk), i_lo);
+      uint32_t i = 0;
+      for (; i < i_lo; ++i) {
+        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+        lo = hi;
+        hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+        block8_multi<W, true, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, 8u * i - (uint32_t)l, c.n, work,
+                                       segmul, k);
+      }
+      for (; i < i_hi; ++i) {
+        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+        lo = hi;
+        hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+        block8_multi<W, false, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, 8u * i - (uint32_t)l, c.n, work,
+                                        segmul, k);
+      }
+      for (; i < nblk; ++i) {
+        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+        lo = hi;
+        hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+        block8_multi<W, true, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, 8u * i - (uint32_t)l, c.n, work,
+                                       segmul, k);
+      }
+#else
       for (uint32_t i = 0; i < nblk; ++i) {
         const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
         lo = hi;
@@ -484,7 +575,8 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
         else
           block8_multi<W, true, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
       }
-      if (work && l == L - 1) in.results[c.id] = make_uint2(kmin & 0xFFFFu, (kmin >> 16) - p);
+#endif
+      if (work && l == L - 1) in.results[c.id] = result_of(in, kmin, p, c.m);
     }
     __syncwarp();
   }
@@ -519,6 +611,250 @@ __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __r
     const uint32_t f = t * nseg;
     const uint32_t cnt = min((uint32_t)nseg, count - f);
     process_tile<W, MULTI, 8, fma_shift<W, MULTI, false>()>(in, ids, first + f, cnt, L, wsmem, lane);
+  }
+}
+
+// ---- Ukkonen's cut-off on single-lane shapes ----
+//
+// With a score bound k per candidate (the cut-off bound of its query), only
+// DP cells of value <= k matter: the minimum is reported only where it is
+// <= k. Cells above every row whose value is <= k can hold anything >= k+1
+// without changing a cell of value <= k (a cell of value <= k is reached only
+// through cells of value <= k), so the rows above that zone need not be
+// computed (Ukkonen 1985; the block form is GEMTools'
+// gt_map_block_bpm_get_distance__cutoff, GEMTools/src/gt_map_align_bpm.c:141-210).
+//
+// Here the rows of a lane's W words form groups of 4 words (128 rows). A
+// warp computes the first Y groups of every column, Y the same for its 32
+// lanes and fixed for each block of 8 columns, so each block runs a code path
+// compiled for its Y: no per-column test. Between blocks each lane works out
+// how many groups it needs:
+//  * gs[g], the value of group g's top row, is kept per column on the FMA
+//    pipe (the top row's Ph/Mh bits, as for the score);
+//  * a row r of group g holds at least (gs[g-1] + gs[g] - 128) / 2 (values
+//    change by at most 1 per row); a group whose bound exceeds k holds no
+//    cell <= k;
+//  * the zone's top row rises by at most one row per column (the cell above
+//    the top row of value <= k holds k + 1, and only a diagonal match from a
+//    cell of value k reaches k again one row up), so over the next 8 columns
+//    the zone stays within the highest group with a cell <= k, plus the next
+//    group when that group's top row is within 8 of k.
+// The warp takes the largest need of its lanes. A group that becomes active
+// starts from the column the warp has reached as the ramp value[r] =
+// value[bottom] + (r - bottom) (Pv all ones, Mv zero): an upper bound of the
+// true values, all of which are > k there, so the argument above applies.
+// The top group holds the query's last row: while it is inactive every score
+// exceeds k and no minimum is taken; when it becomes active the score is its
+// gs. Scores <= k, their first column and the tie-break are exact; a minimum
+// above k is reported as {kNoMatch, kNoMatch} (result_of).
+
+template <int W>
+struct Cut {
+  static_assert(W % 4 == 0 && W >= 8 && W <= 32, "cut-off shapes: 8..32 words, a multiple of 4");
+  static constexpr int G = W / 4;
+};
+
+// One column over the first Y groups. tp / tm: the unshifted top-word Ph / Mh
+// (the last row's horizontal delta) when Y covers every group.
+template <int W, int Y>
+__device__ __forceinline__ void cut_column(const uint32_t* __restrict__ q, uint32_t (&Pv)[W], uint32_t (&Mv)[W],
+                                           uint32_t (&gs)[Cut<W>::G], uint32_t& tp, uint32_t& tm, Mul k) {
+  constexpr int NW = 4 * Y;
+  uint32_t eq[NW];
+#pragma unroll
+  for (int g = 0; g < Y; ++g) {
+    const uint4 v = *reinterpret_cast<const uint4*>(q + g * Layout<W, false>::GROUP);
+    eq[4 * g] = v.x;
+    eq[4 * g + 1] = v.y;
+    eq[4 * g + 2] = v.z;
+    eq[4 * g + 3] = v.w;
+  }
+  uint32_t t[NW], s[NW];
+#pragma unroll
+  for (int j = 0; j < NW; ++j) t[j] = eq[j] & Pv[j];
+  asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(t[0]), "r"(Pv[0]));
+#pragma unroll
+  for (int j = 1; j < NW - 1; ++j) asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s[j]) : "r"(t[j]), "r"(Pv[j]));
+  asm volatile("addc.u32 %0, %1, %2;" : "=r"(s[NW - 1]) : "r"(t[NW - 1]), "r"(Pv[NW - 1]));
+  uint32_t php = 0u, mhp = 0u;
+#pragma unroll
+  for (int j = 0; j < NW; ++j) {
+    const uint32_t pv = Pv[j], mv = Mv[j];
+    const uint32_t xv = eq[j] | mv;
+    const uint32_t xh = (s[j] ^ pv) | eq[j];
+    const uint32_t ph = mv | ~(xh | pv);
+    const uint32_t mh = pv & xh;
+    const uint32_t phs = __funnelshift_l(php, ph, 1);
+    const uint32_t mhs = __funnelshift_l(mhp, mh, 1);
+    Pv[j] = mhs | ~(xv | phs);
+    Mv[j] = phs & xv;
+    php = ph;
+    mhp = mh;
+    if ((j & 3) == 3) {  // the group's top row: +1 / -1 on the FMA pipe
+      const int g = j >> 2;
+      gs[g] = __umulhi(ph, k.two) * k.one + gs[g];
+      gs[g] = __umulhi(mh, k.two) * k.mone + gs[g];
+    }
+  }
+  tp = php;
+  tm = mhp;
+}
+
+// Eight columns with Y active groups; the minimum is taken only when every
+// group is active, for columns < n.
+template <int W, int Y, int UNR>
+__device__ __forceinline__ void cut_block8(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
+                                           uint32_t (&Mv)[W], uint32_t (&gs)[Cut<W>::G], uint32_t& sc,
+                                           uint32_t& kmin, uint32_t colbase, uint32_t n, Mul k) {
+  const uint32_t kb = base_bytes<W, false>(k);
+#pragma unroll UNR
+  for (int u = 0; u < 8; ++u) {
+    const uint32_t code = next_code(t, k);
+    uint32_t tp, tm;
+    cut_column<W, Y>(reinterpret_cast<const uint32_t*>(slot + code * kb), Pv, Mv, gs, tp, tm, k);
+    if constexpr (Y == Cut<W>::G) {
+      sc = key_step(sc, tp, tm, k);
+      if (colbase + (uint32_t)u < n) kmin = min(kmin, sc);
+    }
+  }
+}
+
+// Groups this lane needs for the next 8 columns, from the top-row values of
+// the Y active groups and the bound K (in the padded row layout).
+template <int W, int Y>
+__device__ __forceinline__ int cut_need(const uint32_t (&gs)[Cut<W>::G], int K) {
+  int need = 1;
+  int below = 0;  // row 0
+#pragma unroll
+  for (int g = 0; g < Y; ++g) {
+    const int top = (int)gs[g];
+    if (((below + top - 128) >> 1) <= K) need = g + 1 + (top <= K + 8 ? 1 : 0);
+    below = top;
+  }
+  return need < Cut<W>::G ? need : Cut<W>::G;
+}
+
+// After a block of Y groups: the warp's group count for the next block (at
+// most one more), with a group that becomes active set to the ramp. When the
+// top group becomes active the key takes its score, one column before
+// `colnext`.
+template <int W, int Y>
+__device__ __forceinline__ int cut_next(uint32_t (&Pv)[W], uint32_t (&Mv)[W], uint32_t (&gs)[Cut<W>::G],
+                                        uint32_t& sc, uint32_t colnext, int K, bool active, Mul k) {
+  const int need = active ? cut_need<W, Y>(gs, K) : 1;
+  const int yn = (int)__reduce_max_sync(FULL_MASK, (uint32_t)need);
+  if constexpr (Y < Cut<W>::G) {
+    if (yn > Y) {
+#pragma unroll
+      for (int j = 4 * Y; j < 4 * Y + 4; ++j) {
+        Pv[j] = 0xFFFFFFFFu;
+        Mv[j] = 0u;
+      }
+      gs[Y] = gs[Y - 1] + 128u;
+      if constexpr (Y + 1 == Cut<W>::G) sc = gs[Y] * k.k16 + (colnext - 1u);
+    }
+  }
+  return yn;
+}
+
+template <int W, int UNR, int... Ys>
+__device__ __forceinline__ int cut_dispatch(int y, uint32_t t, const char* slot, uint32_t (&Pv)[W], uint32_t (&Mv)[W],
+                                            uint32_t (&gs)[Cut<W>::G], uint32_t& sc, uint32_t& kmin,
+                                            uint32_t colbase, uint32_t n, int K, bool active, Mul k,
+                                            std::integer_sequence<int, Ys...>) {
+  int yn = y;
+  ((y == Ys + 1 ? (cut_block8<W, Ys + 1, UNR>(t, slot, Pv, Mv, gs, sc, kmin, colbase, n, k),
+                   yn = cut_next<W, Ys + 1>(Pv, Mv, gs, sc, colbase + 8u, K, active, k), 0)
+                : 0),
+   ...);
+  return yn;
+}
+
+#ifndef MYERS_CUTOFF_UNROLL
+#define MYERS_CUTOFF_UNROLL 4
+#endif
+
+// One warp tile of a single-lane shape under the cut-off (the staging and
+// candidate set-up of process_tile). The warp steps its lanes' windows
+// together, to the longest, so that every lane takes part in the group vote.
+template <int W>
+__device__ __forceinline__ void cut_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
+                                         uint32_t cnt, uint32_t* __restrict__ wsmem, int lane) {
+  using Lay = Layout<W, false>;
+  constexpr int G = Cut<W>::G;
+  constexpr int rows = 32 * W;
+  const CandSetup c = setup_candidate(in, ids, first, cnt, lane, 32, 0, rows);
+  const uint32_t qkey = c.has ? c.query : 0xFFFFFFFFu;
+  const uint32_t qprev = __shfl_up_sync(FULL_MASK, qkey, 1);
+  const bool starts = c.has && (lane == 0 || qprev != qkey);
+  const unsigned run_starts = __ballot_sync(FULL_MASK, starts);
+  const int run = __popc(run_starts & (lane >= 31 ? FULL_MASK : ((2u << lane) - 1u))) - 1;
+  const int rounds = (__popc(run_starts) + Lay::SLOTS - 1) / Lay::SLOTS;
+  const uint32_t p = (uint32_t)rows - c.m;
+  const long long q0 = (long long)(in.exact ? c.pos : (c.pos & ~7ull));
+  const long long b0 = q0 >> 3;
+  const uint32_t sh = 4u * (uint32_t)(q0 & 7);
+  const Mul k = make_mul(in);
+
+  for (int r = 0; r < rounds; ++r) {
+    const int slot = run - r * Lay::SLOTS;
+    const bool in_round = c.has && slot >= 0 && slot < Lay::SLOTS;
+    uint32_t* lane_part = wsmem + (in_round ? slot : 0) * 4;
+    if (in_round && starts && c.qok) stage_lane<W, false>(lane_part, in.peq, c.pos_entry, c.m, W, 0);
+    __syncwarp();
+    const bool work = c.work && in_round;
+    const char* slotp = reinterpret_cast<const char*>(lane_part);
+    const int K = work ? (int)(d_cutoff_bound(c.m, in.cutoff) + p) : 0;
+    const uint32_t nblk_lane = work ? (c.n + 7u) >> 3 : 0u;
+    const uint32_t nblk = __reduce_max_sync(FULL_MASK, nblk_lane);
+    if (nblk > 0) {
+      uint32_t Pv[W], Mv[W], gs[G];
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        Pv[j] = 0xFFFFFFFFu;
+        Mv[j] = 0u;
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) gs[g] = 128u * (uint32_t)(g + 1);  // column -1: value[r] = r
+      uint32_t sc = ((uint32_t)rows << 16) - 1u;                       // key counter, column -1
+      uint32_t kmin = (uint32_t)rows << 16;
+      int y = (int)__reduce_max_sync(FULL_MASK, work ? (uint32_t)cut_need<W, G>(gs, K) : 1u);
+      uint32_t lo = ref_load(in.ref, b0, in.ref_words);
+      uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
+      for (uint32_t i = 0; i < nblk; ++i) {
+        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
+        lo = hi;
+        hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
+        y = cut_dispatch<W, MYERS_CUTOFF_UNROLL>(y, t, slotp, Pv, Mv, gs, sc, kmin, 8u * i, c.n, K,
+                                                 i + 1 < nblk_lane, k, std::make_integer_sequence<int, G>{});
+      }
+      if (work) in.results[c.id] = result_of(in, kmin, p, c.m);
+    }
+    __syncwarp();
+  }
+}
+
+// Plain launch of a single-lane shape under the cut-off (the tile loop of
+// k_plain).
+template <int W>
+__global__ void __launch_bounds__(128, 4) k_cutoff(DevInputs in, const uint32_t* __restrict__ ids,
+                                                   const BucketState* __restrict__ st, int cfg, uint32_t first,
+                                                   uint32_t count, int /* L: 1 */, uint32_t* __restrict__ next) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  if (st != nullptr) {
+    first = st->first[cfg];
+    count = st->count[cfg];
+  }
+  uint32_t* wsmem = smem + wib * Layout<W, false>::WORDS;
+  const uint32_t tiles = (count + 31) / 32;
+  while (true) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(next, 1u);
+    t = __shfl_sync(FULL_MASK, t, 0);
+    if (t >= tiles) break;
+    const uint32_t f = t * 32;
+    cut_tile<W>(in, ids, first + f, min(32u, count - f), wsmem, lane);
   }
 }
 
@@ -749,6 +1085,35 @@ cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_id
   return cudaGetLastError();
 }
 
+// Cut-off kernels of the single-lane shapes of 8, 12, ..., 32 words.
+static const PlainFn kCutoffTable[] = {&k_cutoff<8>, &k_cutoff<12>, &k_cutoff<16>, &k_cutoff<20>,
+                                       &k_cutoff<24>, &k_cutoff<28>, &k_cutoff<32>};
+
+bool has_cutoff_kernel(int v) {
+  const int W = variant_W(v);
+  return !variant_multi(v) && W % 4 == 0 && W >= 8 && W <= 32;
+}
+
+cudaError_t launch_cutoff(int v, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state, int cfg,
+                          uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms) {
+  if (!has_cutoff_kernel(v)) return cudaErrorInvalidValue;
+  const PlainFn fn = kCutoffTable[variant_W(v) / 4 - 2];
+  const int threads = 128;
+  const size_t smem = (size_t)warp_smem_bytes(v, 1) * (threads / 32);
+  cudaError_t e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int nb = blocks_per_sm((const void*)fn, threads, smem);
+  uint32_t grid = (uint32_t)(num_sms * nb);
+  if (d_state == nullptr) {
+    const uint32_t tiles = (count + 31) / 32;
+    const uint32_t need = (tiles + threads / 32 - 1) / (threads / 32);
+    if (need < grid) grid = need;
+    if (grid == 0) return cudaSuccess;
+  }
+  fn<<<grid, threads, smem, s>>>(in, d_ids, d_state, cfg, first, count, 1, d_next);
+  return cudaGetLastError();
+}
+
 int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_state, uint8_t* d_cfg_of_cand,
                      uint32_t* d_ids, cudaStream_t s, int num_sms, cudaError_t* err) {
   const int threads = 256;
@@ -775,6 +1140,21 @@ cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const Pla
   if (need < grid) grid = need > 0 ? need : 1;
   k_batched<<<grid, threads, smem, s>>>(in, d_ids, plan, d_state);
   return cudaGetLastError();
+}
+
+cudaError_t load_batched_path_kernels() {
+  cudaFuncAttributes a;
+  const void* fns[] = {(const void*)k_classify, (const void*)k_plan, (const void*)k_scatter, (const void*)k_batched};
+  for (const void* f : fns) {
+    const cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+  }
+  for (int v = 0; v < kNumVariants; ++v) {
+    if (batched_supports(v)) continue;  // shapes the persistent kernel does not carry get plain launches
+    const cudaError_t e = cudaFuncGetAttributes(&a, (const void*)kPlainTable.f[v]);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iters, cudaStream_t s) {

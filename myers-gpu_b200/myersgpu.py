@@ -2,8 +2,8 @@
 
 The product is libmyers_b200.so: CUDA kernels for sm_100a behind the C ABI
 declared in include/myers-interface.h (a drop-in for the reference's
-src-api/myers-interface.h). This module only binds that ABI and the seeded
-workload generator (libmyers_synth.so); there is no Python compute path. If
+src-api/myers-interface.h). This module only binds that ABI, and re-exports the
+seeded workload generator of myerssynth.py; there is no Python compute path. If
 the library is missing, importing this module raises.
 
 Record layouts (numpy dtypes) match the C structs byte for byte:
@@ -17,15 +17,13 @@ import os
 
 import numpy as np
 
+# the record layouts and the seeded workload generator (no CUDA code)
+from myerssynth import (CAND, GENOME, PAD_WORD, QINFO, QRY_ENTRY, RES, SynthSpec, cells,  # noqa: F401
+                        make_reference, make_workload, spec, workload_spec)
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmyers_b200.so")
-SYNTH_PATH = os.path.join(HERE, "libmyers_synth.so")
 
-QRY_ENTRY = np.dtype([("bitmap", "<u4", (5, 4))])
-CAND = np.dtype([("query", "<u4"), ("pad", "<u4"), ("position", "<u8")])
-QINFO = np.dtype([("posEntry", "<u4"), ("size", "<u4")])
-RES = np.dtype([("column", "<u4"), ("score", "<u4")])
-assert QRY_ENTRY.itemsize == 80 and CAND.itemsize == 16 and QINFO.itemsize == 8 and RES.itemsize == 8
 
 SUCCESS = 0
 E_OPENING_FILE, E_READING_FILE, E_INSUFFICIENT_MEM_GPU, E_ALLOCATE_MEM, E_INCOMPATIBLE_GPU = 1, 2, 3, 4, 5
@@ -33,6 +31,7 @@ E_INVALID_ARGUMENT, E_CAPACITY, E_QUERY_TOO_LONG, E_CUDA, E_TIMEOUT, E_NOT_READY
 WINDOW_ALIGNED, WINDOW_EXACT = 0, 1
 PATH_PLAIN, PATH_BATCHED = 0, 1
 NO_RESULT = 0xFFFFFFFF
+NO_MATCH = 0xFFFFFFFF  # column and score of a candidate above the cut-off bound
 MAX_QUERY_BASES = 32768
 NOALLOC_MAX_CANDIDATES = 262144
 
@@ -50,7 +49,6 @@ def _load(path):
 
 
 lib = _load(LIB_PATH)
-synth = _load(SYNTH_PATH)
 
 _P, _U32, _U64, _I32, _F = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_float
 _PP = C.POINTER(C.c_void_p)
@@ -87,6 +85,9 @@ _sig("myersContextCreate", _I32, _PP, _U64)
 _sig("myersContextDestroy", _I32, _P)
 _sig("myersVerifyAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _P, _P)
 _sig("myersVerifyRangeAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _U32, _U32, _P, _P)
+_sig("myersVerifyCutoffAsync", _I32, _P, _P, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _I32, _F, _U32, _U32, _P,
+     _P)
+_sig("myersSetCutoff", _I32, _P, _F)
 _sig("myersVerifyNoAllocAsync", _I32, _P, _U64, _U64, _P, _U32, _P, _U32, _P, _U32, _F, _I32, _U32, _U32, _P, _P)
 _sig("myersContextLastLaunches", _U32, _P)
 _sig("myersPackPEQAsync", _I32, _P, _P, _U64, _P, _P, _U32, _P, _U32, _P)
@@ -119,7 +120,7 @@ EXPORTED = (
     "myersGetErrorString myersInit myersSend myersReceive myersEnd myersSetWindowMode "
     "myersSetKernelPath myersSetGraphs myersSetMemoryBudget myersGetDevice myersGetLastStatus myersReferenceCreate "
     "myersReferenceLoad myersReferenceDestroy myersReferenceSize myersContextCreate myersContextDestroy "
-    "myersVerifyAsync myersVerifyRangeAsync myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
+    "myersVerifyAsync myersVerifyRangeAsync myersVerifyCutoffAsync myersSetCutoff myersVerifyNoAllocAsync myersContextLastLaunches myersContextFlags "
     "myersPackPEQAsync myersPackReferenceAsync "
     "myersBufferLastLaunches myersNumVariants myersVariantWords myersVariantIsMulti myersShapeOf "
     "myersSetShapeOverride myersTunedShapes myersProbeIntPeak myersServerCreate myersServerSubmit myersServerPoll myersServerWait "
@@ -208,6 +209,11 @@ class Buffers:
         for h in (self.handles if i is None else [self.handles[i]]):
             check(lib.myersSetKernelPath(h, path), "myersSetKernelPath")
 
+    def set_cutoff(self, cutoff, i=None):
+        """Ukkonen's cut-off for the next sends (None: off)."""
+        for h in (self.handles if i is None else [self.handles[i]]):
+            check(lib.myersSetCutoff(h, -1.0 if cutoff is None else cutoff), "myersSetCutoff")
+
     def set_graphs(self, enable, i=None):
         for h in (self.handles if i is None else [self.handles[i]]):
             check(lib.myersSetGraphs(h, int(bool(enable))), "myersSetGraphs")
@@ -274,8 +280,14 @@ class Context:
         check(lib.myersContextCreate(C.byref(self.h), max_candidates), "myersContextCreate")
 
     def verify(self, ref, d_peq, n_entries, d_qinfo, n_queries, d_cands, n_cands, distance, d_results,
-               window=WINDOW_ALIGNED, path=PATH_PLAIN, stream=0, min_size=0, max_size=0):
-        """Enqueue on `stream` (a cudaStream_t as int). Pointers are device addresses."""
+               window=WINDOW_ALIGNED, path=PATH_PLAIN, stream=0, min_size=0, max_size=0, cutoff=None):
+        """Enqueue on `stream` (a cudaStream_t as int). Pointers are device
+        addresses. `cutoff` (a fraction of the query length) selects Ukkonen's
+        cut-off (myersVerifyCutoffAsync)."""
+        if cutoff is not None:
+            return check(lib.myersVerifyCutoffAsync(self.h, ref.h, d_peq, n_entries, d_qinfo, n_queries, d_cands,
+                                                    n_cands, distance, window, path, cutoff, min_size, max_size,
+                                                    d_results, stream), "myersVerifyCutoffAsync")
         return check(lib.myersVerifyRangeAsync(self.h, ref.h, d_peq, n_entries, d_qinfo, n_queries, d_cands, n_cands,
                                                distance, window, path, min_size, max_size, d_results, stream),
                      "myersVerifyRangeAsync")
@@ -349,7 +361,7 @@ def traceback_torch(tb, ref, peq, qinfo, cands, results, distance, max_score, ma
 
 
 def verify_torch(ctx, ref, peq, qinfo, cands, distance, window=WINDOW_ALIGNED, path=PATH_PLAIN, min_size=0,
-                 max_size=0, device="cuda"):
+                 max_size=0, device="cuda", cutoff=None):
     """Copy numpy inputs to the GPU with torch, verify, return numpy results."""
     import torch
 
@@ -360,7 +372,8 @@ def verify_torch(ctx, ref, peq, qinfo, cands, distance, window=WINDOW_ALIGNED, p
     d_res = torch.empty(len(cands) * RES.itemsize, dtype=torch.uint8, device=device)
     stream = torch.cuda.current_stream().cuda_stream
     ctx.verify(ref, d_peq.data_ptr(), len(peq), d_qi.data_ptr(), len(qinfo), d_c.data_ptr(), len(cands), distance,
-               d_res.data_ptr(), window=window, path=path, stream=stream, min_size=min_size, max_size=max_size)
+               d_res.data_ptr(), window=window, path=path, stream=stream, min_size=min_size, max_size=max_size,
+               cutoff=cutoff)
     torch.cuda.synchronize()
     return d_res.cpu().numpy().view(RES)
 
@@ -439,133 +452,3 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
-
-
-# ---------------------------------------------------------------------------
-# synthetic workloads
-
-
-class SynthSpec(C.Structure):
-    _fields_ = [
-        ("ref_size", C.c_uint64), ("num_reads", C.c_uint32),
-        ("len_kind", C.c_uint32), ("len_fixed", C.c_uint32), ("len_lo", C.c_uint32), ("len_hi", C.c_uint32),
-        ("len_set_n", C.c_uint32), ("len_set", C.c_uint32 * 16), ("len_weights", C.c_double * 16),
-        ("mut_kind", C.c_uint32), ("sub", C.c_double), ("ins", C.c_double), ("del_", C.c_double),
-        ("rate_lo", C.c_double), ("rate_hi", C.c_double), ("indel_mean", C.c_double),
-        ("cand_kind", C.c_uint32), ("cand_fixed", C.c_uint32), ("cand_lambda", C.c_double),
-        ("cand_cap", C.c_uint32), ("cand_lo", C.c_uint32), ("cand_hi", C.c_uint32),
-        ("jitter", C.c_uint32), ("distance", C.c_float), ("seed", C.c_uint64),
-    ]
-
-
-synth.synth_reference.restype = C.c_int
-synth.synth_reference.argtypes = [C.c_uint64, C.c_double, C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p, C.c_uint64]
-synth.synth_plan.restype = C.c_int
-synth.synth_plan.argtypes = [C.POINTER(SynthSpec), C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
-                             C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
-synth.synth_fill.restype = C.c_int
-synth.synth_fill.argtypes = [C.POINTER(SynthSpec), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                             C.c_void_p, C.c_void_p, C.c_void_p]
-
-PAD_WORD = 0x44444444
-
-
-def make_reference(size, seed, n_frac=0.001, run=(50, 500), pad_words=0):
-    """Packed reference of `size` bases (i.i.d. ACGT with N runs); returns the
-    ceil(size/8) words plus `pad_words` words of N."""
-    nw = (size + 7) // 8 + pad_words
-    words = np.empty(nw, dtype=np.uint32)
-    rc = synth.synth_reference(size, n_frac, run[0], run[1], seed, words.ctypes.data, nw)
-    if rc:
-        raise RuntimeError(f"synth_reference failed ({rc})")
-    return words
-
-
-def spec(ref_size, num_reads, seed, distance=0.2, lengths=100, length_weights=None, length_range=None,
-         uniform_lengths=None, sub=0.04, ins=0.005, dele=0.005, rate_range=None, indel_mean=1.0, cands=11,
-         cand_poisson=None, cand_cap=0, cand_range=None, jitter=8):
-    s = SynthSpec()
-    s.ref_size, s.num_reads, s.seed, s.distance, s.jitter = ref_size, num_reads, seed, distance, jitter
-    if length_range is not None:
-        s.len_kind, s.len_lo, s.len_hi = 2, length_range[0], length_range[1]
-    elif uniform_lengths is not None:
-        s.len_kind, s.len_set_n = 3, len(uniform_lengths)
-        for i, v in enumerate(uniform_lengths):
-            s.len_set[i] = v
-    elif length_weights is not None:
-        s.len_kind, s.len_set_n = 1, len(lengths)
-        for i, (v, w) in enumerate(zip(lengths, length_weights)):
-            s.len_set[i], s.len_weights[i] = v, w
-    else:
-        s.len_kind, s.len_fixed = 0, lengths
-    if rate_range is not None:
-        s.mut_kind, s.rate_lo, s.rate_hi = 1, rate_range[0], rate_range[1]
-    else:
-        s.mut_kind, s.sub, s.ins, s.del_ = 0, sub, ins, dele
-    s.indel_mean = indel_mean
-    if cand_poisson is not None:
-        s.cand_kind, s.cand_lambda, s.cand_cap = 1, cand_poisson, cand_cap
-    elif cand_range is not None:
-        s.cand_kind, s.cand_lo, s.cand_hi = 2, cand_range[0], cand_range[1]
-    else:
-        s.cand_kind, s.cand_fixed = 0, cands
-    return s
-
-
-def make_workload(s, ref_words, ascii=False):
-    """Reads and candidates for spec `s` over `ref_words`. Returns a dict with
-    peq (QRY_ENTRY), qinfo (QINFO), cands (CAND), lengths, ncands, true_pos
-    and, if asked, the reads as one ASCII byte string (bases back to back)."""
-    n = s.num_reads
-    lengths = np.empty(n, dtype=np.uint32)
-    ncands = np.empty(n, dtype=np.uint32)
-    te, tc, tb = C.c_uint64(), C.c_uint64(), C.c_uint64()
-    synth.synth_plan(C.byref(s), lengths.ctypes.data, ncands.ctypes.data, C.byref(te), C.byref(tc), C.byref(tb))
-    peq = np.empty(te.value, dtype=QRY_ENTRY)
-    qinfo = np.empty(n, dtype=QINFO)
-    cands = np.empty(tc.value, dtype=CAND)
-    true_pos = np.empty(n, dtype=np.uint64)
-    asc = np.empty(tb.value, dtype=np.uint8) if ascii else None
-    rc = synth.synth_fill(C.byref(s), ref_words.ctypes.data, lengths.ctypes.data, ncands.ctypes.data,
-                          qinfo.ctypes.data, peq.ctypes.data, cands.ctypes.data,
-                          asc.ctypes.data if ascii else None, true_pos.ctypes.data)
-    if rc:
-        raise RuntimeError(f"synth_fill failed ({rc})")
-    out = dict(peq=peq, qinfo=qinfo, cands=cands, lengths=lengths, ncands=ncands, true_pos=true_pos)
-    if ascii:
-        out["ascii"] = asc
-    return out
-
-
-# The workloads of the benchmark, by number. `scale` shrinks the read count
-# (and, for the 16 Mbase one, nothing else) for tests.
-GENOME = 3_100_000_000
-
-
-def workload_spec(k, seed=None, scale=1.0, ref_size=None):
-    if k == 1:
-        return spec(ref_size or 16_000_000, max(1, int(100_000 * scale)), seed or 101, lengths=100,
-                    sub=0.04, ins=0.005, dele=0.005, cands=11)
-    if k == 2:
-        return spec(ref_size or GENOME, max(1, int(1_000_000 * scale)), seed or 202, lengths=1000,
-                    sub=0.05, ins=0.005, dele=0.005, cands=11)
-    if k == 3:
-        return spec(ref_size or GENOME, max(1, int(2_000_000 * scale)), seed or 303,
-                    lengths=[100, 200, 400, 600, 800, 1000], length_weights=[30, 20, 15, 15, 10, 10],
-                    rate_range=(0.02, 0.08), cand_poisson=10.0, cand_cap=64)
-    if k == 4:
-        return spec(ref_size or GENOME, max(1, int(100_000 * scale)), seed or 404, length_range=(1000, 10000),
-                    sub=0.03, ins=0.06, dele=0.03, indel_mean=1.5, cand_poisson=4.0)
-    if k == 5:
-        return spec(ref_size or GENOME, max(1, int(100_000 * scale)), seed or 505,
-                    uniform_lengths=list(range(100, 1001, 100)), rate_range=(0.02, 0.08), cand_range=(1, 64))
-    raise ValueError(k)
-
-
-def cells(qinfo, cands, distance=0.2, exact=False):
-    """DP cells (m x columns) of the candidates, as the throughput unit."""
-    m = qinfo["size"][cands["query"]].astype(np.float64)
-    f = np.float32(1.0) + np.float32(2.0) * np.float32(distance)
-    w = np.floor(m.astype(np.float32) * f).astype(np.float64)
-    n = w if exact else 8 * (np.floor(w / 8) + np.where(w % 8 != 0, 2, 1))
-    return m * n, np.ceil(m / 32) * n

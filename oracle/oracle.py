@@ -19,10 +19,11 @@ PAD_WORD = 0x44444444
 RES = np.dtype([("column", "<u4"), ("score", "<u4")])
 
 
-def build():
-    """Compile the oracle (and, where the reference sources exist, _ref/)."""
+def build(ref_src=None):
+    """Compile the oracle (and _ref/, when `ref_src` names a checkout of the
+    reference's sources)."""
     import subprocess
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE] + ([f"REF={ref_src}"] if ref_src else []), check=True)
 
 
 def _lib(name, required=True):
@@ -69,6 +70,31 @@ def verify(peq, qinfo, cands, ref_words, ref_size, distance, exact=False, nthrea
     _orc.orc_verify(peq.ctypes.data, qinfo.ctypes.data, cands.ctypes.data, len(cands), ref_words.ctypes.data,
                     ref_words.size, ref_size, distance, int(exact), res.ctypes.data, nthreads)
     return res
+
+
+NO_RESULT = 0xFFFFFFFF
+NO_MATCH = 0xFFFFFFFF
+
+
+def cutoff_bound(m, cutoff):
+    """The cut-off bound of queries of m bases: (uint32_t)(m * cutoff) with
+    the product in float32 (the window sizing's convention)."""
+    return np.floor(np.asarray(m, dtype=np.float32) * np.float32(cutoff)).astype(np.int64)
+
+
+def apply_cutoff(results, qinfo, cands, cutoff):
+    """The cut-off contract on full results: a verified candidate whose
+    minimum score exceeds the bound of its query becomes {NO_MATCH, NO_MATCH};
+    everything else is unchanged. The contract of GEMTools'
+    gt_map_block_bpm_get_distance__cutoff (GEMTools/src/gt_map_align_bpm.c:
+    141-210), which returns a distance and position only within its
+    max_distance, on results pinned to the reference's CPU Myers."""
+    out = np.array(results, copy=True)
+    m = qinfo["size"][cands["query"]]
+    sel = (out["score"] != NO_RESULT) & (out["score"].astype(np.int64) > cutoff_bound(m, cutoff))
+    out["column"][sel] = NO_MATCH
+    out["score"][sel] = NO_MATCH
+    return out
 
 
 def traceback(peq, qinfo, cands, results, ref_words, ref_size, distance, max_score, max_ops, exact=False,
@@ -128,20 +154,25 @@ def have_reference():
     return _pad is not None and _exa is not None
 
 
-def _padded(ref_words):
-    # the reference reads up to two words past the packed array; give it N
+def pad_reference(ref_words):
+    """The packed reference followed by 16 words of N: the reference's CPU
+    code reads up to two words past the packed array. Callers that check
+    several batches against one reference pass this to the calls below
+    (`padded=`) instead of having each call copy the reference."""
     return np.concatenate([np.asarray(ref_words, dtype=np.uint32), np.full(16, PAD_WORD, dtype=np.uint32)])
 
 
-def reference_verify_aligned(peq, qinfo, cands, ref_words, ref_size, distance, nthreads=0, uncapped=True):
+def reference_verify_aligned(peq, qinfo, cands, ref_words, ref_size, distance, nthreads=0, uncapped=True,
+                             padded=None):
     """The reference's computeAllQueriesCPU (aligned window). Returns
-    (results, seconds of its compute region)."""
+    (results, seconds of its compute region, including the direct
+    computeMyers calls of the reads beyond its 4096-base cap)."""
     if _pad is None:
         raise RuntimeError("oracle/_ref/libref_padding.so is not built")
     peq = np.ascontiguousarray(peq)
     qinfo = np.ascontiguousarray(qinfo)
     cands = np.ascontiguousarray(cands)
-    w = _padded(ref_words)
+    w = pad_reference(ref_words) if padded is None else padded
     res = np.empty(len(cands), dtype=RES)
     sec = C.c_double()
     rc = _pad.refshim_verify_aligned(peq.ctypes.data, len(peq), qinfo.ctypes.data, len(qinfo), cands.ctypes.data,
@@ -152,14 +183,14 @@ def reference_verify_aligned(peq, qinfo, cands, ref_words, ref_size, distance, n
     return res, sec.value
 
 
-def reference_verify_exact(peq, qinfo, cands, ref_words, ref_size, distance, nthreads=0):
+def reference_verify_exact(peq, qinfo, cands, ref_words, ref_size, distance, nthreads=0, padded=None):
     """The reference's exact-window CPU Myers (one query length only)."""
     if _exa is None:
         raise RuntimeError("oracle/_ref/libref_exact.so is not built")
     peq = np.ascontiguousarray(peq)
     qinfo = np.ascontiguousarray(qinfo)
     cands = np.ascontiguousarray(cands)
-    w = _padded(ref_words)
+    w = pad_reference(ref_words) if padded is None else padded
     res = np.empty(len(cands), dtype=RES)
     sec = C.c_double()
     rc = _exa.refshim_verify_exact(peq.ctypes.data, qinfo.ctypes.data, len(qinfo), cands.ctypes.data, len(cands),

@@ -30,7 +30,8 @@
  *   uncapped if non-zero, candidates whose query exceeds the driver's
  *            4096-base cap (:200) are computed by calling computeMyers
  *            directly with the same per-candidate sizing (:192-198)
- *   seconds  wall time of the computeAllQueriesCPU region
+ *   seconds  wall time of the computeAllQueriesCPU region plus, with
+ *            `uncapped`, the direct computeMyers calls after it
  *
  * Returns 0, or -1 if a position does not fit the oracle's 32-bit field.
  */
@@ -82,9 +83,6 @@ int refshim_verify_aligned(qryEntry_t *peq, uint32_t num_entries,
     {
         computeAllQueriesCPU(&r, &q, &rs);
     }
-    double t1 = omp_get_wtime();
-    if (seconds) *seconds = t1 - t0;
-
     if (uncapped) {
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
         for (int64_t i = 0; i < (int64_t)num_cands; ++i) {
@@ -101,6 +99,8 @@ int refshim_verify_aligned(qryEntry_t *peq, uint32_t num_entries,
                          numEntriesPerCandidate);
         }
     }
+    double t1 = omp_get_wtime();
+    if (seconds) *seconds = t1 - t0;
     free(c8);
     return 0;
 }

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
 Run where the reference sources are present (they are compiled into
-oracle/_ref/ by `make -C oracle`):
+oracle/_ref/ by `make -C oracle REF=<reference checkout>`):
 
     python tests/golden/make_golden.py
 
@@ -159,7 +159,7 @@ def verify_fixture(rng):
 
 def main():
     if not orc.have_reference():
-        sys.exit("oracle/_ref is not built (make -C oracle with the reference sources present)")
+        sys.exit("oracle/_ref is not built (make -C oracle REF=<reference checkout>)")
     rng = np.random.default_rng(20241203)
     with tempfile.TemporaryDirectory() as tmp:
         np.savez_compressed(os.path.join(HERE, "packers.npz"), **packers(rng, tmp))

@@ -221,3 +221,20 @@ def test_oracle_traceback_matches_textbook(orc, mg, exact):
     bad["score"] += 1
     aln1, _ = orc.traceback(peq, qinfo, c, bad, words, ref_size, 0.2, 10 ** 6, 16, exact=exact)
     assert (aln1["num_ops"] == orc.TB_INCONSISTENT).all()
+
+
+def test_cutoff_contract_on_reference_outputs(mg, orc, golden_verify):
+    """apply_cutoff keeps every result whose score is within (uint32)(m *
+    cutoff) (float32) and marks the others, leaving unverified candidates
+    ({0, 0xFFFFFFFF}) as they are."""
+    g = golden_verify
+    res = g["res_aligned"]
+    m = g["qinfo"]["size"][g["cands"]["query"]]
+    for cutoff in (0.0, 0.05, 0.2, 2.0):
+        out = orc.apply_cutoff(res, g["qinfo"], g["cands"], cutoff)
+        for i in range(0, len(res), 7):
+            bound = int(np.float32(int(m[i])) * np.float32(cutoff))
+            if res[i]["score"] == orc.NO_RESULT or res[i]["score"] <= bound:
+                assert out[i] == res[i]
+            else:
+                assert out[i]["score"] == orc.NO_MATCH and out[i]["column"] == orc.NO_MATCH

@@ -1,7 +1,6 @@
 """The entry point that allocates nothing (myersVerifyNoAllocAsync), for
-callers that cannot call cudaMalloc -- code running under CUDA graph capture,
-programs whose allocator owns all device memory, services with a frozen
-memory budget. Called through the C ABI on two batches in a row, its results
+callers that cannot call cudaMalloc -- programs whose own allocator owns all
+device memory, services whose memory budget is fixed once they run. Called through the C ABI on two batches in a row, its results
 must equal those of the allocating entry point (myersVerifyRangeAsync, batched
 path) bit for bit: integer outputs, no tolerance. This file is collected last
 so a stop-at-first-failure run has run every other test before it."""
