@@ -27,7 +27,8 @@ JSON line (rank 0).
   configs   (1 GPU, default workload) the other configurations, each with its
             own timing, clocks, roofline fraction and reference parity sample:
             plain-100b, batched-mixed (batched and plain, full size and a
-            110K-candidate batch), batched-long, and a short serving sweep
+            110K-candidate batch), batched-long, plain-1000b under Ukkonen's
+            cut-off, and a short serving sweep
 
 --impl reference times the reference's own CPU implementation instead (the
 GPU path of the reference targets sm_20..sm_50 only).
@@ -537,20 +538,20 @@ def run_ours(args):
 
 
 def config_record(mg, ms, ref, w, path, steps, warmup, peak, ref_words, ref_size, threads, padded, parity_frac,
-                  seed):
+                  seed, cutoff=None):
     """One configuration's figures: device-resident candidates/s with its
     clocks, the roofline fraction, and a reference parity sample whose time
     is the CPU baseline."""
     n = len(w["cands"])
     cells, ws = workload_units(ms, w)
-    r = device_run(mg, ref, w, path, steps, warmup)
+    r = device_run(mg, ref, w, path, steps, warmup, cutoff=cutoff)
     t = float(np.mean(r["step_ms"])) / 1e3
     rec = {"path": "batched" if path == mg.PATH_BATCHED else "plain", "candidates": n, "value": n / t,
            "unit": "candidates/s", "ms_per_step": t * 1e3, "steps": steps, "warmup": warmup, "gcups": cells / t / 1e9,
            "roofline_frac": roofline(peak, ws, t)["frac"], "launches_per_step": r["launches"], "clocks": r["clocks"]}
     if parity_frac > 0:
         rec["parity_sample"], rec["cpu_baseline"] = reference_parity(w, r["res"], ref_words, ref_size, parity_frac,
-                                                                     seed, threads, padded)
+                                                                     seed, threads, padded, cutoff)
     return rec, r["res"]
 
 
@@ -620,6 +621,15 @@ def run_configs(mg, ms, args, ref3, peak, tmp, threads, padded3):
                            "batched_over_plain": b4["value"] / p4["value"]}
     del w4, resb, resp
 
+    # plain-1000b under Ukkonen's cut-off at 0.08 m: the two-pass plain path
+    # (its roofline fraction counts the full DP's word-steps, so it can exceed 1)
+    _, _, _, w2 = make_inputs(ms, 2, 1.0, 0)
+    cut, _ = config_record(mg, ms, ref3, w2, mg.PATH_PLAIN, steps, warmup, peak, rw, rs, threads, padded3, 0.02,
+                           205, cutoff=0.08)
+    out["plain-1000b-cutoff-0.08"] = {"workload": WORKLOAD_NAMES[2] + ", Ukkonen's cut-off at 0.08 m",
+                                      "cutoff": 0.08, **cut}
+    del w2
+
     # serving: a short sweep around the knee
     out["serving"] = serving_sweep(mg, ms, args, ref3, rw, rs, SERVING_RATES_SHORT, steps=min(steps, 5),
                                    warmup=warmup, threads=threads, padded=padded3)
@@ -637,6 +647,7 @@ def north_star_summary(value_plain_1000b, configs):
             + [r["e2e"]["results_equal_device"] for r in records if "results_equal_device" in (r.get("e2e") or {})]
             + [sv["results_equal_to_batched"]])
     return {
+        "cutoff_0.08_over_plain_1000b": configs["plain-1000b-cutoff-0.08"]["value"] / value_plain_1000b,
         "batched_over_plain_mixed_full": configs["batched-mixed"]["batched_over_plain"],
         "batched_over_plain_mixed_110k": configs["batched-mixed-110k"]["batched_over_plain"],
         "batched_over_plain_long": configs["batched-long"]["batched_over_plain"],

@@ -132,6 +132,7 @@ extern "C" int myersReferenceCreate(myersReference_t** ref, const uint32_t* host
 // fread returns, myersGPU.c:117-122).
 extern "C" int myersReferenceLoad(myersReference_t** ref, const char* fileName) {
   if (ref == nullptr || fileName == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  NvtxRange range("myers: reference load");
   FILE* fp = fopen(fileName, "rb");
   if (fp == nullptr) return MYERS_E_OPENING_FILE;
   uint32_t hdr[2];
@@ -394,9 +395,61 @@ extern "C" int myersContextDestroy(myersContext_t* c) {
   cudaFree(c->d_cfg);
   cudaFree(c->d_state);
   cudaFree(c->d_flags);
+  cudaFree(c->d_esc_ids);
+  cudaFree(c->d_esc_cfg);
+  cudaFree(c->d_esc_state);
   cudaSetDevice(cur);
   delete c;
   return MYERS_SUCCESS;
+}
+
+int myers::ensure_cutoff_scratch(myersContext* c) {
+  if (c->d_esc_ids != nullptr) return MYERS_SUCCESS;
+  const size_t n = c->capacity ? c->capacity : 1;
+  cudaError_t e = cudaMalloc((void**)&c->d_esc_ids, n * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_esc_cfg, n);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_esc_state, sizeof(BucketState));
+  if (e != cudaSuccess) {
+    cudaFree(c->d_esc_ids);
+    cudaFree(c->d_esc_cfg);
+    cudaFree(c->d_esc_state);
+    c->d_esc_ids = nullptr;
+    c->d_esc_cfg = nullptr;
+    c->d_esc_state = nullptr;
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? MYERS_E_INSUFFICIENT_MEM_GPU : cuda_fail(e, "cut-off scratch");
+  }
+  return MYERS_SUCCESS;
+}
+
+float myers::cutoff_prefix_mult() {
+  static const float mult = [] {
+    const char* env = getenv("MYERS_CUTOFF_PREFIX");
+    const float v = env ? strtof(env, nullptr) : 0.0f;
+    return v > 0.0f ? v : 2.0f;
+  }();
+  return mult;
+}
+
+uint32_t myers::host_prefix_rows(uint32_t m, float cutoff, float mult) {
+  const uint32_t k = (uint32_t)((float)m * cutoff);
+  const float r = mult * (float)k;
+  const uint32_t rows = r >= 65536.0f ? 0xFFFFFFFFu : (((uint32_t)r + 63u) & ~31u);
+  return rows < m ? rows : m;
+}
+
+int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float mult) {
+  uint8_t w1[kMaxWords + 1], w2[kMaxWords + 1];
+  memset(w1, 0, sizeof(w1));
+  memset(w2, 0, sizeof(w2));
+  for (uint32_t m = 1; m <= kMaxWords * 32; ++m) {
+    if (!present_m[m]) continue;
+    const uint32_t r = host_prefix_rows(m, cutoff, mult);
+    w1[(r + 31) / 32] = 1;
+    if (r < m) w2[(m + 31) / 32] = 1;
+  }
+  const int st = build_plan(plan, w1, false);
+  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, false);
 }
 
 extern "C" uint32_t myersContextLastLaunches(const myersContext_t* c) { return c ? c->last_launches : 0; }
@@ -417,7 +470,7 @@ uint32_t myers::batched_tile_bound(const PlanTable& plan, uint32_t n) {
 }
 
 int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in0, const PlanTable& plan,
-                          int path, cudaStream_t s) {
+                          int path, cudaStream_t s, const PlanTable* plan2) {
   DevInputs in = in0;
   in.ref = ref->d_words;
   in.ref_size = ref->size;
@@ -431,14 +484,53 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     // no query needs the DP (all empty or all too long): classify alone
     // writes every result
   }
-  // a plain launch of shape c: under the cut-off, the single-lane shapes
-  // that have a cut-off kernel skip the rows above the band
   auto plain = [&](uint32_t c, const uint32_t* ids, const BucketState* st, uint32_t count, uint32_t* next) {
     const Shape sh = plan.shape[c];
-    if (in.cut && has_cutoff_kernel(sh.variant))
-      return launch_cutoff(sh.variant, in, ids, st, (int)c, 0, count, next, s, ctx->num_sms);
     return launch_plain(sh.variant, sh.L, in, ids, st, (int)c, 0, count, next, s, ctx->num_sms);
   };
+  if (in.cut && path == MYERS_PATH_PLAIN && plan2 != nullptr) {
+    // Ukkonen's cut-off in two passes. The first runs every candidate's DP
+    // on a prefix of its query (plan: the prefixes' shapes) and settles the
+    // candidates whose prefix minimum exceeds the bound; the others are
+    // appended to lists by full-length shape (plan2), and the second pass
+    // runs their full queries.
+    if (ctx->d_esc_ids == nullptr) return MYERS_E_INVALID_ARGUMENT;  // ensure_cutoff_scratch first
+    in.prefix = 1;
+    in.esc_ids = ctx->d_esc_ids;
+    in.esc_state = ctx->d_esc_state;
+    CU(cudaMemsetAsync(ctx->d_esc_state, 0, sizeof(BucketState), s));
+    uint32_t launches = 0;
+    if (plan.num_cfg <= 1 && plan2->num_cfg <= 1) {
+      in.esc_cfg = nullptr;  // one full-length shape: list 0
+      if (plan.num_cfg == 1) {
+        uint32_t* next = &ctx->d_state->next[0];
+        CU(cudaMemsetAsync(next, 0, sizeof(uint32_t), s));
+        CU(plain(0, nullptr, nullptr, in.num_cands, next));
+        ++launches;
+      }
+    } else {
+      in.esc_cfg = ctx->d_esc_cfg;
+      CU(cudaMemsetAsync(ctx->d_state, 0, sizeof(BucketState), s));
+      cudaError_t e = cudaSuccess;
+      launches += (uint32_t)launch_bucketing_cutoff(in, plan, *plan2, ctx->d_state, ctx->d_cfg, ctx->d_ids, s,
+                                                    ctx->num_sms, &e);
+      if (e != cudaSuccess) return cuda_fail(e, "bucketing");
+      for (uint32_t c = 0; c < plan.num_cfg; ++c) {
+        CU(plain(c, ctx->d_ids, ctx->d_state, 0, &ctx->d_state->next[c]));
+        ++launches;
+      }
+    }
+    DevInputs in2 = in;
+    in2.prefix = 0;
+    for (uint32_t c = 0; c < plan2->num_cfg; ++c) {
+      const Shape sh = plan2->shape[c];
+      CU(launch_plain(sh.variant, sh.L, in2, ctx->d_esc_ids, ctx->d_esc_state, (int)c, 0, 0,
+                      &ctx->d_esc_state->next[c], s, ctx->num_sms));
+      ++launches;
+    }
+    ctx->last_launches = launches;
+    return MYERS_SUCCESS;
+  }
   if (path == MYERS_PATH_PLAIN && plan.num_cfg == 1) {
     uint32_t* next = &ctx->d_state->next[0];  // the launch's tile counter
     CU(cudaMemsetAsync(next, 0, sizeof(uint32_t), s));
@@ -520,15 +612,28 @@ static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const 
                         void* stream) {
   if (ctx == nullptr || ref == nullptr) return MYERS_E_INVALID_ARGUMENT;
   if (!(distance >= 0.0f) || !std::isfinite(distance)) return MYERS_E_INVALID_ARGUMENT;
+  NvtxRange range("myers: verify (enqueue)");
   if (windowMode != MYERS_WINDOW_ALIGNED && windowMode != MYERS_WINDOW_EXACT) return MYERS_E_INVALID_ARGUMENT;
   if (path != MYERS_PATH_PLAIN && path != MYERS_PATH_BATCHED) return MYERS_E_INVALID_ARGUMENT;
   if (numCandidates > 0 && (d_peq == nullptr || d_qinfo == nullptr || d_cands == nullptr || d_results == nullptr))
     return MYERS_E_INVALID_ARGUMENT;
-  PlanTable plan;
-  int st = plan_for_range(plan, minQuerySize, maxQuerySize, path);
+  PlanTable plan, plan2;
+  const bool two_pass = cutoff >= 0.0f && path == MYERS_PATH_PLAIN;
+  const float mult = cutoff_prefix_mult();
+  int st;
+  if (two_pass) {
+    std::vector<uint8_t> present_m(kMaxWords * 32 + 1, 0);
+    const uint32_t hi = (maxQuerySize == 0 || maxQuerySize > kMaxWords * 32) ? kMaxWords * 32 : maxQuerySize;
+    for (uint32_t m = minQuerySize ? minQuerySize : 1; m <= hi; ++m) present_m[m] = 1;
+    st = cutoff_plans(plan, plan2, present_m.data(), cutoff, mult);
+    if (st == MYERS_SUCCESS) st = ensure_cutoff_scratch(ctx);
+  } else {
+    st = plan_for_range(plan, minQuerySize, maxQuerySize, path);
+  }
   if (st != MYERS_SUCCESS) return st;
   DevInputs in;
   memset(&in, 0, sizeof(in));
+  in.prefix_mult = mult;
   in.peq = reinterpret_cast<const uint32_t*>(d_peq);
   in.qinfo = reinterpret_cast<const uint2*>(d_qinfo);
   in.cands = reinterpret_cast<const Cand*>(d_cands);
@@ -540,7 +645,7 @@ static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const 
   in.exact = windowMode == MYERS_WINDOW_EXACT;
   in.cut = cutoff >= 0.0f;
   in.cutoff = in.cut ? cutoff : 0.0f;
-  return verify_enqueue(ctx, ref, in, plan, path, (cudaStream_t)stream);
+  return verify_enqueue(ctx, ref, in, plan, path, (cudaStream_t)stream, two_pass ? &plan2 : nullptr);
 }
 
 extern "C" int myersContextFlags(myersContext_t* ctx, uint32_t* flags, int clear) {
@@ -710,8 +815,9 @@ struct Buffer {
   cudaGraphExec_t exec;  // the last send, updated in place by the next
   int last_status;
   bool pending;
-  std::vector<uint8_t> present;  // word counts of the last send
-  PlanTable plan;
+  std::vector<uint8_t> present;    // word counts of the last send
+  std::vector<uint8_t> present_m;  // query lengths of the last send (cut-off only)
+  PlanTable plan, plan2;
   bool plan_valid;
   int plan_path;
 };
@@ -848,6 +954,7 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
   if (!(distance >= 0.0f) || !std::isfinite(distance)) return b->last_status = MYERS_E_INVALID_ARGUMENT;
   if (numPEQEntries > b->maxPEQEntries || numQueries > b->maxQueries || numCandidates > b->maxCandidates)
     return b->last_status = MYERS_E_CAPACITY;
+  NvtxRange range("myers: send");
   CU(cudaSetDevice(b->device));
   // O(queries) host pass: the word counts present pick the shapes
   std::vector<uint8_t>& present = b->present;
@@ -857,7 +964,22 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
     if (m > 0 && m <= kMaxWords * 32) present[(m + 31) / 32] = 1;  // longer: flagged on the device
   }
   PlanTable& plan = b->plan;
-  int st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
+  const bool two_pass = b->cutoff >= 0.0f && b->path == MYERS_PATH_PLAIN;
+  int st;
+  {
+    NvtxRange plan_range("myers: send: shape plan");
+    if (two_pass) {
+      std::vector<uint8_t>& pm = b->present_m;
+      pm.assign(kMaxWords * 32 + 1, 0);
+      for (uint32_t q = 0; q < numQueries; ++q) {
+        const uint32_t m = b->h_qinfo[q].size;
+        if (m > 0 && m <= kMaxWords * 32) pm[m] = 1;
+      }
+      st = cutoff_plans(plan, b->plan2, pm.data(), b->cutoff, cutoff_prefix_mult());
+    } else {
+      st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
+    }
+  }
   if (st != MYERS_SUCCESS) return b->last_status = st;
   cudaStream_t s = b->stream;
   auto enqueue = [&]() -> int {
@@ -885,7 +1007,8 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
     in.exact = b->window_mode == MYERS_WINDOW_EXACT;
     in.cut = b->cutoff >= 0.0f;
     in.cutoff = in.cut ? b->cutoff : 0.0f;
-    const int est = verify_enqueue(b->ctx, b->shared->ref, in, plan, b->path, s);
+    in.prefix_mult = cutoff_prefix_mult();
+    const int est = verify_enqueue(b->ctx, b->shared->ref, in, plan, b->path, s, two_pass ? &b->plan2 : nullptr);
     if (est != MYERS_SUCCESS) return est;
     CU(cudaMemcpyAsync(b->h_results, b->d_results, (size_t)numCandidates * sizeof(resEntry_t),
                        cudaMemcpyDeviceToHost, s));
@@ -906,6 +1029,7 @@ extern "C" void sendMyersBuffer(void* mb, float distance, uint32_t numPEQEntries
 extern "C" int myersReceive(void* mb) {
   Buffer* b = static_cast<Buffer*>(mb);
   if (b == nullptr) return MYERS_E_INVALID_ARGUMENT;
+  NvtxRange range("myers: receive (stream sync)");
   CU(cudaSetDevice(b->device));
   CU(cudaStreamSynchronize(b->stream));
   if (b->pending) {
@@ -946,6 +1070,11 @@ extern "C" int myersSetKernelPath(void* mb, int path) {
 extern "C" int myersSetCutoff(void* mb, float cutoff) {
   Buffer* b = static_cast<Buffer*>(mb);
   if (b == nullptr || std::isnan(cutoff) || std::isinf(cutoff)) return MYERS_E_INVALID_ARGUMENT;
+  if (cutoff >= 0.0f) {
+    CU(cudaSetDevice(b->device));
+    const int st = ensure_cutoff_scratch(b->ctx);
+    if (st != MYERS_SUCCESS) return st;
+  }
   b->cutoff = cutoff < 0.0f ? -1.0f : cutoff;
   return MYERS_SUCCESS;
 }

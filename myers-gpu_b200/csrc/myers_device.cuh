@@ -18,6 +18,21 @@ __device__ __forceinline__ uint32_t d_window_bases(uint32_t m, float distance) {
 
 __device__ __forceinline__ uint32_t d_window_words(uint32_t wb) { return wb / 8 + ((wb % 8) ? 2u : 1u); }
 
+// The cut-off bound of a query of m bases: (uint32_t)(m * cutoff) in float32.
+__device__ __forceinline__ uint32_t d_cutoff_bound(uint32_t m, float cutoff) {
+  return (uint32_t)__fmul_rn((float)m, cutoff);
+}
+
+// Rows of the cut-off's first pass for a query of m bases with bound k: k
+// times the multiplier (float32, truncated), plus 32, rounded up to whole
+// 32-row words, at most m. The same arithmetic as host_prefix_rows.
+__device__ __forceinline__ uint32_t d_prefix_rows(uint32_t m, float cutoff, float mult) {
+  const uint32_t k = d_cutoff_bound(m, cutoff);
+  const float r = __fmul_rn(mult, (float)k);
+  const uint32_t rows = r >= 65536.0f ? 0xFFFFFFFFu : (((uint32_t)r + 63u) & ~31u);
+  return rows < m ? rows : m;
+}
+
 // Reference codes 5..7 behave as A (code 0) and bit 3 is ignored, as in the
 // reference kernel's select (src-api/coreMyersGPU-CC50.cu:82-95, :170).
 __device__ __forceinline__ uint32_t sanitize_codes(uint32_t t) {

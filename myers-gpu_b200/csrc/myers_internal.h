@@ -3,8 +3,19 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 namespace myers {
+
+// An NVTX range over a scope: host stages show up by name on a profiler's
+// timeline (nsys, ncu's NVTX filters); without a tool attached a push/pop is
+// a check of a null callback.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Eight N codes: what the kernels read past the end of the packed reference.
 constexpr uint32_t kPadWord = 0x44444444u;
@@ -93,9 +104,20 @@ struct DevInputs {
   float distance;
   int exact;
   // Ukkonen cut-off: with `cut` set, a candidate whose minimum score exceeds
-  // (uint32_t)(m * cutoff) (float32) gets {kNoMatch, kNoMatch}.
+  // its bound k = (uint32_t)(m * cutoff) (float32) gets {kNoMatch, kNoMatch}.
   float cutoff;
   int cut;
+  // The cut-off's first pass (prefix set): the DP runs on the first
+  // prefix_rows(m) rows of each query only (prefix_rows in myers_device.cuh).
+  // A candidate whose prefix minimum exceeds k cannot come within k and gets
+  // {kNoMatch, kNoMatch}; the others are appended to esc_ids (shape
+  // esc_cfg[id] of the second pass, or shape 0 without esc_cfg) for a second
+  // pass over their full queries.
+  int prefix;
+  float prefix_mult;
+  uint32_t* esc_ids;
+  struct BucketState* esc_state;
+  uint8_t* esc_cfg;
   // Multipliers the compiler cannot fold (set by set_multipliers): they keep
   // the per-column bookkeeping on the FMA pipe (see myers_kernels.cu).
   uint32_t one, two, k16, mk16, p28, kb33, kb17, mn16, mone;
@@ -130,12 +152,14 @@ int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_
 cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state,
                          int cfg, uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms);
 
-// Whether the plain path has a cut-off kernel for variant v (single-lane
-// shapes of 8..32 words, a multiple of 4), and one launch of it; arguments
-// as launch_plain.
-bool has_cutoff_kernel(int v);
-cudaError_t launch_cutoff(int v, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state, int cfg,
-                          uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms);
+// The cut-off's bucketing: classify by the first pass's (prefix) shapes
+// under `plan` and, for the candidates a prefix covers only in part, by their
+// full-length shapes under `plan2` (into in.esc_cfg, counted in
+// in.esc_state->cursor); then lay out both. d_state and in.esc_state must be
+// zeroed first. Returns launches.
+int launch_bucketing_cutoff(const DevInputs& in, const PlanTable& plan, const PlanTable& plan2,
+                            BucketState* d_state, uint8_t* d_cfg_of_cand, uint32_t* d_ids, cudaStream_t s,
+                            int num_sms, cudaError_t* err);
 
 // The persistent batched launch over the plan's first num_batched shapes;
 // the grid is the device's resident capacity or, for small batches, one
@@ -191,12 +215,31 @@ struct myersContext {
   myers::BucketState* d_state;
   uint32_t* d_flags;
   uint32_t last_launches;
+  // the cut-off's second pass (allocated at the first cut-off request)
+  uint32_t* d_esc_ids;
+  uint8_t* d_esc_cfg;
+  myers::BucketState* d_esc_state;
 };
 
 namespace myers {
 // Enqueue the kernels of one batch on stream s (inputs already on the device).
+// With in.cut on the plain path the cut-off runs in two passes: `plan` must
+// then hold the first pass's (prefix) shapes and `plan2` the full-length
+// shapes (cutoff_plans).
 int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in, const PlanTable& plan, int path,
-                   cudaStream_t s);
+                   cudaStream_t s, const PlanTable* plan2 = nullptr);
+// The cut-off's plans from the word counts of the full queries present: the
+// first pass's prefix shapes into `plan`, the full-length shapes into
+// `plan2`. `present_m[m]` flags each query length m (1..kMaxWords*32).
+int cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float prefix_mult);
+// The first pass's rows of a query of m bases (as prefix_rows on the device).
+uint32_t host_prefix_rows(uint32_t m, float cutoff, float prefix_mult);
+// Device scratch of the cut-off's second pass for a context (once).
+int ensure_cutoff_scratch(myersContext* ctx);
+// The multiplier of the first pass's rows (MYERS_CUTOFF_PREFIX, default 2:
+// the fastest of 1, 1.5, 2, 2.5, 3 and 4 on 1,000-base reads at bounds of
+// 0.04 to 0.2 of m).
+float cutoff_prefix_mult();
 
 // Capture what enqueue() puts on stream s and launch it as the graph *exec.
 // Consecutive batches differ only in copy sizes and kernel arguments, so the

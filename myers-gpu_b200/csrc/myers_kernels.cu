@@ -367,11 +367,6 @@ __device__ __forceinline__ void block8_multi(uint32_t t, const char* __restrict_
   }
 }
 
-// The cut-off bound of a query of m bases: (uint32_t)(m * cutoff) in float32.
-__device__ __forceinline__ uint32_t d_cutoff_bound(uint32_t m, float cutoff) {
-  return (uint32_t)__fmul_rn((float)m, cutoff);
-}
-
 // The result of a verified candidate from its (score << 16 | column) key,
 // whose score carries the p padding rows. Under the cut-off contract a
 // minimum above the bound is reported as {kNoMatch, kNoMatch}.
@@ -379,6 +374,27 @@ __device__ __forceinline__ uint2 result_of(const DevInputs& in, uint32_t kmin, u
   const uint32_t score = (kmin >> 16) - p;
   if (in.cut && score > d_cutoff_bound(m, in.cutoff)) return make_uint2(kNoMatch, kNoMatch);
   return make_uint2(kmin & 0xFFFFu, score);
+}
+
+// Finish a candidate whose DP ran over rows m of its query of mf bases. On a
+// prefix (the cut-off's first pass, m < mf): every path to the query's last
+// row crosses row m, at a cost of at least the prefix minimum, so a prefix
+// minimum above the bound k settles the candidate as no match (Ukkonen's
+// cut-off); otherwise it goes to the second pass, appended to its full shape's
+// list.
+__device__ __forceinline__ void finish(const DevInputs& in, uint32_t id, uint32_t kmin, uint32_t p, uint32_t m,
+                                       uint32_t mf) {
+  if (m < mf) {
+    if ((kmin >> 16) - p > d_cutoff_bound(mf, in.cutoff)) {
+      in.results[id] = make_uint2(kNoMatch, kNoMatch);
+    } else {
+      const uint32_t cfg = in.esc_cfg ? in.esc_cfg[id] : 0u;
+      const uint32_t k = atomicAdd(&in.esc_state->count[cfg], 1u);
+      in.esc_ids[in.esc_state->first[cfg] + k] = id;
+    }
+  } else {
+    in.results[id] = result_of(in, kmin, p, m);
+  }
 }
 
 // Multi-lane shapes: run the pipeline's ramp-up, steady state and drain as
@@ -392,7 +408,8 @@ struct CandSetup {
   uint32_t id;
   uint32_t query;
   unsigned long long pos;
-  uint32_t m;
+  uint32_t m;     // rows of the DP: the query's length, or the cut-off's first-pass prefix of it
+  uint32_t mf;    // the query's length
   uint32_t pos_entry;
   uint32_t n;     // columns
   bool has;       // the segment holds a candidate
@@ -419,6 +436,7 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
   c.id = 0;
   c.pos = 0;
   c.m = 0;
+  c.mf = 0;
   c.pos_entry = 0;
   c.n = 0;
   c.query = 0;
@@ -434,8 +452,9 @@ __device__ __forceinline__ CandSetup setup_candidate(const DevInputs& in, const 
     c.query = cd.query;
     c.pos = cd.position;
     c.pos_entry = q.x;
-    c.m = q.y;
-    const uint32_t wb = d_window_bases(c.m, in.distance);
+    c.mf = q.y;
+    c.m = in.prefix ? d_prefix_rows(c.mf, in.cutoff, in.prefix_mult) : c.mf;
+    const uint32_t wb = d_window_bases(c.mf, in.distance);
     const bool valid = bad == 0u && c.pos < in.ref_size && (in.ref_size - c.pos) > (unsigned long long)wb;
     c.n = in.exact ? wb : 8u * d_window_words(wb);
     const bool fits = c.m <= (uint32_t)rows && c.n <= kMaxColumns;
@@ -524,7 +543,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
           const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
           block8_single<W, true, UNR, FS>(t, slotp, Pv, Mv, sc, kmin, 8u * i, c.n, k);
         }
-        in.results[c.id] = result_of(in, kmin, p, c.m);
+        finish(in, c.id, kmin, p, c.m, c.mf);
       }
     } else {
       uint32_t steps = work ? c.n + (uint32_t)L - 1u : 0u;
@@ -576,7 +595,7 @@ __device__ __forceinline__ void process_tile(const DevInputs& in, const uint32_t
           block8_multi<W, true, UNR, FS>(t, slotp, Pv, Mv, outP, outM, sc, kmin, jbase, c.n, work, segmul, k);
       }
 #endif
-      if (work && l == L - 1) in.results[c.id] = result_of(in, kmin, p, c.m);
+      if (work && l == L - 1) finish(in, c.id, kmin, p, c.m, c.mf);
     }
     __syncwarp();
   }
@@ -614,253 +633,15 @@ __global__ void __launch_bounds__(128) k_plain(DevInputs in, const uint32_t* __r
   }
 }
 
-// ---- Ukkonen's cut-off on single-lane shapes ----
-//
-// With a score bound k per candidate (the cut-off bound of its query), only
-// DP cells of value <= k matter: the minimum is reported only where it is
-// <= k. Cells above every row whose value is <= k can hold anything >= k+1
-// without changing a cell of value <= k (a cell of value <= k is reached only
-// through cells of value <= k), so the rows above that zone need not be
-// computed (Ukkonen 1985; the block form is GEMTools'
-// gt_map_block_bpm_get_distance__cutoff, GEMTools/src/gt_map_align_bpm.c:141-210).
-//
-// Here the rows of a lane's W words form groups of 4 words (128 rows). A
-// warp computes the first Y groups of every column, Y the same for its 32
-// lanes and fixed for each block of 8 columns, so each block runs a code path
-// compiled for its Y: no per-column test. Between blocks each lane works out
-// how many groups it needs:
-//  * gs[g], the value of group g's top row, is kept per column on the FMA
-//    pipe (the top row's Ph/Mh bits, as for the score);
-//  * a row r of group g holds at least (gs[g-1] + gs[g] - 128) / 2 (values
-//    change by at most 1 per row); a group whose bound exceeds k holds no
-//    cell <= k;
-//  * the zone's top row rises by at most one row per column (the cell above
-//    the top row of value <= k holds k + 1, and only a diagonal match from a
-//    cell of value k reaches k again one row up), so over the next 8 columns
-//    the zone stays within the highest group with a cell <= k, plus the next
-//    group when that group's top row is within 8 of k.
-// The warp takes the largest need of its lanes. A group that becomes active
-// starts from the column the warp has reached as the ramp value[r] =
-// value[bottom] + (r - bottom) (Pv all ones, Mv zero): an upper bound of the
-// true values, all of which are > k there, so the argument above applies.
-// The top group holds the query's last row: while it is inactive every score
-// exceeds k and no minimum is taken; when it becomes active the score is its
-// gs. Scores <= k, their first column and the tie-break are exact; a minimum
-// above k is reported as {kNoMatch, kNoMatch} (result_of).
-
-template <int W>
-struct Cut {
-  static_assert(W % 4 == 0 && W >= 8 && W <= 32, "cut-off shapes: 8..32 words, a multiple of 4");
-  static constexpr int G = W / 4;
-};
-
-// One column over the first Y groups. tp / tm: the unshifted top-word Ph / Mh
-// (the last row's horizontal delta) when Y covers every group.
-template <int W, int Y>
-__device__ __forceinline__ void cut_column(const uint32_t* __restrict__ q, uint32_t (&Pv)[W], uint32_t (&Mv)[W],
-                                           uint32_t (&gs)[Cut<W>::G], uint32_t& tp, uint32_t& tm, Mul k) {
-  constexpr int NW = 4 * Y;
-  uint32_t eq[NW];
-#pragma unroll
-  for (int g = 0; g < Y; ++g) {
-    const uint4 v = *reinterpret_cast<const uint4*>(q + g * Layout<W, false>::GROUP);
-    eq[4 * g] = v.x;
-    eq[4 * g + 1] = v.y;
-    eq[4 * g + 2] = v.z;
-    eq[4 * g + 3] = v.w;
-  }
-  uint32_t t[NW], s[NW];
-#pragma unroll
-  for (int j = 0; j < NW; ++j) t[j] = eq[j] & Pv[j];
-  asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s[0]) : "r"(t[0]), "r"(Pv[0]));
-#pragma unroll
-  for (int j = 1; j < NW - 1; ++j) asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s[j]) : "r"(t[j]), "r"(Pv[j]));
-  asm volatile("addc.u32 %0, %1, %2;" : "=r"(s[NW - 1]) : "r"(t[NW - 1]), "r"(Pv[NW - 1]));
-  uint32_t php = 0u, mhp = 0u;
-#pragma unroll
-  for (int j = 0; j < NW; ++j) {
-    const uint32_t pv = Pv[j], mv = Mv[j];
-    const uint32_t xv = eq[j] | mv;
-    const uint32_t xh = (s[j] ^ pv) | eq[j];
-    const uint32_t ph = mv | ~(xh | pv);
-    const uint32_t mh = pv & xh;
-    const uint32_t phs = __funnelshift_l(php, ph, 1);
-    const uint32_t mhs = __funnelshift_l(mhp, mh, 1);
-    Pv[j] = mhs | ~(xv | phs);
-    Mv[j] = phs & xv;
-    php = ph;
-    mhp = mh;
-    if ((j & 3) == 3) {  // the group's top row: +1 / -1 on the FMA pipe
-      const int g = j >> 2;
-      gs[g] = __umulhi(ph, k.two) * k.one + gs[g];
-      gs[g] = __umulhi(mh, k.two) * k.mone + gs[g];
-    }
-  }
-  tp = php;
-  tm = mhp;
-}
-
-// Eight columns with Y active groups; the minimum is taken only when every
-// group is active, for columns < n.
-template <int W, int Y, int UNR>
-__device__ __forceinline__ void cut_block8(uint32_t t, const char* __restrict__ slot, uint32_t (&Pv)[W],
-                                           uint32_t (&Mv)[W], uint32_t (&gs)[Cut<W>::G], uint32_t& sc,
-                                           uint32_t& kmin, uint32_t colbase, uint32_t n, Mul k) {
-  const uint32_t kb = base_bytes<W, false>(k);
-#pragma unroll UNR
-  for (int u = 0; u < 8; ++u) {
-    const uint32_t code = next_code(t, k);
-    uint32_t tp, tm;
-    cut_column<W, Y>(reinterpret_cast<const uint32_t*>(slot + code * kb), Pv, Mv, gs, tp, tm, k);
-    if constexpr (Y == Cut<W>::G) {
-      sc = key_step(sc, tp, tm, k);
-      if (colbase + (uint32_t)u < n) kmin = min(kmin, sc);
-    }
-  }
-}
-
-// Groups this lane needs for the next 8 columns, from the top-row values of
-// the Y active groups and the bound K (in the padded row layout).
-template <int W, int Y>
-__device__ __forceinline__ int cut_need(const uint32_t (&gs)[Cut<W>::G], int K) {
-  int need = 1;
-  int below = 0;  // row 0
-#pragma unroll
-  for (int g = 0; g < Y; ++g) {
-    const int top = (int)gs[g];
-    if (((below + top - 128) >> 1) <= K) need = g + 1 + (top <= K + 8 ? 1 : 0);
-    below = top;
-  }
-  return need < Cut<W>::G ? need : Cut<W>::G;
-}
-
-// After a block of Y groups: the warp's group count for the next block (at
-// most one more), with a group that becomes active set to the ramp. When the
-// top group becomes active the key takes its score, one column before
-// `colnext`.
-template <int W, int Y>
-__device__ __forceinline__ int cut_next(uint32_t (&Pv)[W], uint32_t (&Mv)[W], uint32_t (&gs)[Cut<W>::G],
-                                        uint32_t& sc, uint32_t colnext, int K, bool active, Mul k) {
-  const int need = active ? cut_need<W, Y>(gs, K) : 1;
-  const int yn = (int)__reduce_max_sync(FULL_MASK, (uint32_t)need);
-  if constexpr (Y < Cut<W>::G) {
-    if (yn > Y) {
-#pragma unroll
-      for (int j = 4 * Y; j < 4 * Y + 4; ++j) {
-        Pv[j] = 0xFFFFFFFFu;
-        Mv[j] = 0u;
-      }
-      gs[Y] = gs[Y - 1] + 128u;
-      if constexpr (Y + 1 == Cut<W>::G) sc = gs[Y] * k.k16 + (colnext - 1u);
-    }
-  }
-  return yn;
-}
-
-template <int W, int UNR, int... Ys>
-__device__ __forceinline__ int cut_dispatch(int y, uint32_t t, const char* slot, uint32_t (&Pv)[W], uint32_t (&Mv)[W],
-                                            uint32_t (&gs)[Cut<W>::G], uint32_t& sc, uint32_t& kmin,
-                                            uint32_t colbase, uint32_t n, int K, bool active, Mul k,
-                                            std::integer_sequence<int, Ys...>) {
-  int yn = y;
-  ((y == Ys + 1 ? (cut_block8<W, Ys + 1, UNR>(t, slot, Pv, Mv, gs, sc, kmin, colbase, n, k),
-                   yn = cut_next<W, Ys + 1>(Pv, Mv, gs, sc, colbase + 8u, K, active, k), 0)
-                : 0),
-   ...);
-  return yn;
-}
-
-#ifndef MYERS_CUTOFF_UNROLL
-#define MYERS_CUTOFF_UNROLL 4
-#endif
-
-// One warp tile of a single-lane shape under the cut-off (the staging and
-// candidate set-up of process_tile). The warp steps its lanes' windows
-// together, to the longest, so that every lane takes part in the group vote.
-template <int W>
-__device__ __forceinline__ void cut_tile(const DevInputs& in, const uint32_t* __restrict__ ids, uint32_t first,
-                                         uint32_t cnt, uint32_t* __restrict__ wsmem, int lane) {
-  using Lay = Layout<W, false>;
-  constexpr int G = Cut<W>::G;
-  constexpr int rows = 32 * W;
-  const CandSetup c = setup_candidate(in, ids, first, cnt, lane, 32, 0, rows);
-  const uint32_t qkey = c.has ? c.query : 0xFFFFFFFFu;
-  const uint32_t qprev = __shfl_up_sync(FULL_MASK, qkey, 1);
-  const bool starts = c.has && (lane == 0 || qprev != qkey);
-  const unsigned run_starts = __ballot_sync(FULL_MASK, starts);
-  const int run = __popc(run_starts & (lane >= 31 ? FULL_MASK : ((2u << lane) - 1u))) - 1;
-  const int rounds = (__popc(run_starts) + Lay::SLOTS - 1) / Lay::SLOTS;
-  const uint32_t p = (uint32_t)rows - c.m;
-  const long long q0 = (long long)(in.exact ? c.pos : (c.pos & ~7ull));
-  const long long b0 = q0 >> 3;
-  const uint32_t sh = 4u * (uint32_t)(q0 & 7);
-  const Mul k = make_mul(in);
-
-  for (int r = 0; r < rounds; ++r) {
-    const int slot = run - r * Lay::SLOTS;
-    const bool in_round = c.has && slot >= 0 && slot < Lay::SLOTS;
-    uint32_t* lane_part = wsmem + (in_round ? slot : 0) * 4;
-    if (in_round && starts && c.qok) stage_lane<W, false>(lane_part, in.peq, c.pos_entry, c.m, W, 0);
-    __syncwarp();
-    const bool work = c.work && in_round;
-    const char* slotp = reinterpret_cast<const char*>(lane_part);
-    const int K = work ? (int)(d_cutoff_bound(c.m, in.cutoff) + p) : 0;
-    const uint32_t nblk_lane = work ? (c.n + 7u) >> 3 : 0u;
-    const uint32_t nblk = __reduce_max_sync(FULL_MASK, nblk_lane);
-    if (nblk > 0) {
-      uint32_t Pv[W], Mv[W], gs[G];
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-        Pv[j] = 0xFFFFFFFFu;
-        Mv[j] = 0u;
-      }
-#pragma unroll
-      for (int g = 0; g < G; ++g) gs[g] = 128u * (uint32_t)(g + 1);  // column -1: value[r] = r
-      uint32_t sc = ((uint32_t)rows << 16) - 1u;                       // key counter, column -1
-      uint32_t kmin = (uint32_t)rows << 16;
-      int y = (int)__reduce_max_sync(FULL_MASK, work ? (uint32_t)cut_need<W, G>(gs, K) : 1u);
-      uint32_t lo = ref_load(in.ref, b0, in.ref_words);
-      uint32_t hi = ref_load(in.ref, b0 + 1, in.ref_words);
-      for (uint32_t i = 0; i < nblk; ++i) {
-        const uint32_t t = sanitize_codes(__funnelshift_r(lo, hi, sh));
-        lo = hi;
-        hi = ref_load(in.ref, b0 + (long long)i + 2, in.ref_words);
-        y = cut_dispatch<W, MYERS_CUTOFF_UNROLL>(y, t, slotp, Pv, Mv, gs, sc, kmin, 8u * i, c.n, K,
-                                                 i + 1 < nblk_lane, k, std::make_integer_sequence<int, G>{});
-      }
-      if (work) in.results[c.id] = result_of(in, kmin, p, c.m);
-    }
-    __syncwarp();
-  }
-}
-
-// Plain launch of a single-lane shape under the cut-off (the tile loop of
-// k_plain).
-template <int W>
-__global__ void __launch_bounds__(128, 4) k_cutoff(DevInputs in, const uint32_t* __restrict__ ids,
-                                                   const BucketState* __restrict__ st, int cfg, uint32_t first,
-                                                   uint32_t count, int /* L: 1 */, uint32_t* __restrict__ next) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  if (st != nullptr) {
-    first = st->first[cfg];
-    count = st->count[cfg];
-  }
-  uint32_t* wsmem = smem + wib * Layout<W, false>::WORDS;
-  const uint32_t tiles = (count + 31) / 32;
-  while (true) {
-    uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(next, 1u);
-    t = __shfl_sync(FULL_MASK, t, 0);
-    if (t >= tiles) break;
-    const uint32_t f = t * 32;
-    cut_tile<W>(in, ids, first + f, min(32u, count - f), wsmem, lane);
-  }
-}
-
 // ---- length bucketing on the device ----
 
-__global__ void k_classify(DevInputs in, const __grid_constant__ PlanTable plan, BucketState* st,
+// With TWO (the cut-off's first pass) a candidate is classified by its
+// prefix's word count under `plan`, and, when the prefix covers only part of
+// its query, by its full word count under `plan2` into in.esc_cfg, counted in
+// in.esc_state->cursor (the second pass's layout).
+template <bool TWO>
+__global__ void k_classify(DevInputs in, const __grid_constant__ PlanTable plan,
+                           const __grid_constant__ PlanTable plan2, BucketState* st,
                            uint8_t* __restrict__ cfg_of_cand) {
   const int lane = threadIdx.x & 31;
   const uint32_t n = in.num_cands;
@@ -873,8 +654,9 @@ __global__ void k_classify(DevInputs in, const __grid_constant__ PlanTable plan,
       uint2 q = make_uint2(0u, 0u);
       if (cd.query < in.num_queries) q = __ldg(in.qinfo + cd.query);
       const uint32_t bad = check_query(in, cd.query, q);
-      const uint32_t m = q.y;
-      const uint32_t wb = d_window_bases(m, in.distance);
+      const uint32_t mf = q.y;
+      const uint32_t m = TWO ? d_prefix_rows(mf, in.cutoff, in.prefix_mult) : mf;
+      const uint32_t wb = d_window_bases(mf, in.distance);
       const bool valid = bad == 0u && cd.position < in.ref_size &&
                          (in.ref_size - cd.position) > (unsigned long long)wb;
       const uint32_t ncol = in.exact ? wb : 8u * d_window_words(wb);
@@ -885,16 +667,36 @@ __global__ void k_classify(DevInputs in, const __grid_constant__ PlanTable plan,
         in.results[i] = make_uint2(0u, kNoResult);
       } else if (m == 0) {
         in.results[i] = make_uint2(0u, 0u);
-      } else if (m > kMaxWords * 32 || ncol > kMaxColumns || plan.cfg_of_words[(m + 31) >> 5] == kNoCfg) {
+      } else if (mf > kMaxWords * 32 || ncol > kMaxColumns || plan.cfg_of_words[(m + 31) >> 5] == kNoCfg ||
+                 (TWO && m < mf && plan2.cfg_of_words[(mf + 31) >> 5] == kNoCfg)) {
         in.results[i] = make_uint2(0u, kNoResult);
         atomicOr(in.flags, kFlagUnsupported);
       } else {
         cfg = plan.cfg_of_words[(m + 31) >> 5];
+        if (TWO && m < mf) {
+          const uint32_t c2 = plan2.cfg_of_words[(mf + 31) >> 5];
+          in.esc_cfg[i] = (uint8_t)c2;
+          atomicAdd(&in.esc_state->cursor[c2], 1u);
+        }
       }
       cfg_of_cand[i] = (uint8_t)cfg;
     }
     const unsigned peers = __match_any_sync(FULL_MASK, cfg);
     if (cfg != kNoCfg && lane == __ffs(peers) - 1) atomicAdd(&st->count[cfg], (uint32_t)__popc(peers));
+  }
+}
+
+// The second pass's layout: each full-length shape's list starts where the
+// candidates counted for it in the classification end up at most; the lists
+// fill as the first pass appends to them.
+__global__ void k_plan_escalation(const __grid_constant__ PlanTable plan2, BucketState* esc) {
+  if (threadIdx.x != 0) return;
+  uint32_t acc = 0;
+  for (uint32_t c = 0; c < plan2.num_cfg; ++c) {
+    esc->first[c] = acc;
+    acc += esc->cursor[c];
+    esc->count[c] = 0;
+    esc->next[c] = 0;
   }
 }
 
@@ -1085,46 +887,32 @@ cudaError_t launch_plain(int v, int L, const DevInputs& in, const uint32_t* d_id
   return cudaGetLastError();
 }
 
-// Cut-off kernels of the single-lane shapes of 8, 12, ..., 32 words.
-static const PlainFn kCutoffTable[] = {&k_cutoff<8>, &k_cutoff<12>, &k_cutoff<16>, &k_cutoff<20>,
-                                       &k_cutoff<24>, &k_cutoff<28>, &k_cutoff<32>};
-
-bool has_cutoff_kernel(int v) {
-  const int W = variant_W(v);
-  return !variant_multi(v) && W % 4 == 0 && W >= 8 && W <= 32;
-}
-
-cudaError_t launch_cutoff(int v, const DevInputs& in, const uint32_t* d_ids, const BucketState* d_state, int cfg,
-                          uint32_t first, uint32_t count, uint32_t* d_next, cudaStream_t s, int num_sms) {
-  if (!has_cutoff_kernel(v)) return cudaErrorInvalidValue;
-  const PlainFn fn = kCutoffTable[variant_W(v) / 4 - 2];
-  const int threads = 128;
-  const size_t smem = (size_t)warp_smem_bytes(v, 1) * (threads / 32);
-  cudaError_t e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int nb = blocks_per_sm((const void*)fn, threads, smem);
-  uint32_t grid = (uint32_t)(num_sms * nb);
-  if (d_state == nullptr) {
-    const uint32_t tiles = (count + 31) / 32;
-    const uint32_t need = (tiles + threads / 32 - 1) / (threads / 32);
-    if (need < grid) grid = need;
-    if (grid == 0) return cudaSuccess;
-  }
-  fn<<<grid, threads, smem, s>>>(in, d_ids, d_state, cfg, first, count, 1, d_next);
-  return cudaGetLastError();
-}
-
 int launch_bucketing(const DevInputs& in, const PlanTable& plan, BucketState* d_state, uint8_t* d_cfg_of_cand,
                      uint32_t* d_ids, cudaStream_t s, int num_sms, cudaError_t* err) {
   const int threads = 256;
   const uint32_t need = (in.num_cands + threads - 1) / threads;
   uint32_t grid = (uint32_t)num_sms * 8;
   if (need < grid) grid = need > 0 ? need : 1;
-  k_classify<<<grid, threads, 0, s>>>(in, plan, d_state, d_cfg_of_cand);
+  k_classify<false><<<grid, threads, 0, s>>>(in, plan, plan, d_state, d_cfg_of_cand);
   k_plan<<<1, 32, 0, s>>>(plan, d_state);
   k_scatter<<<grid, threads, 0, s>>>(in.num_cands, d_cfg_of_cand, d_state, d_ids);
   *err = cudaGetLastError();
   return 3;
+}
+
+int launch_bucketing_cutoff(const DevInputs& in, const PlanTable& plan, const PlanTable& plan2,
+                            BucketState* d_state, uint8_t* d_cfg_of_cand, uint32_t* d_ids, cudaStream_t s,
+                            int num_sms, cudaError_t* err) {
+  const int threads = 256;
+  const uint32_t need = (in.num_cands + threads - 1) / threads;
+  uint32_t grid = (uint32_t)num_sms * 8;
+  if (need < grid) grid = need > 0 ? need : 1;
+  k_classify<true><<<grid, threads, 0, s>>>(in, plan, plan2, d_state, d_cfg_of_cand);
+  k_plan<<<1, 32, 0, s>>>(plan, d_state);
+  k_plan_escalation<<<1, 32, 0, s>>>(plan2, in.esc_state);
+  k_scatter<<<grid, threads, 0, s>>>(in.num_cands, d_cfg_of_cand, d_state, d_ids);
+  *err = cudaGetLastError();
+  return 4;
 }
 
 cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,
@@ -1144,7 +932,8 @@ cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const Pla
 
 cudaError_t load_batched_path_kernels() {
   cudaFuncAttributes a;
-  const void* fns[] = {(const void*)k_classify, (const void*)k_plan, (const void*)k_scatter, (const void*)k_batched};
+  const void* fns[] = {(const void*)k_classify<false>, (const void*)k_plan, (const void*)k_scatter,
+                       (const void*)k_batched};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncGetAttributes(&a, f);
     if (e != cudaSuccess) return e;

@@ -131,6 +131,7 @@ static int enqueue_batch(myersServer* srv, Slot& s, const PlanTable& plan, uint3
 // dispatcher thread without the lock (the slot and its requests are owned by
 // the dispatcher until it is pushed on the in-flight queue).
 static int dispatch_slot(myersServer* srv, Slot& s) {
+  NvtxRange range("myers server: pack and launch a batch");
   uint8_t present[kMaxWords + 1];
   memset(present, 0, sizeof(present));
   uint32_t ne = 0, nq = 0, nc = 0;
@@ -265,13 +266,20 @@ static void completer_main(myersServer* srv) {
     srv->inflight.pop_front();
     Slot& s = srv->slots[si];
     lk.unlock();
-    const cudaError_t e = cudaEventSynchronize(s.done);
+    cudaError_t e;
+    {
+      NvtxRange range("myers server: wait for a batch");
+      e = cudaEventSynchronize(s.done);
+    }
     const uint64_t t = now_ns();
     uint32_t off = 0;
-    for (Request* r : s.reqs) {
-      const size_t n = r->pos.size();
-      r->res.assign(s.h_res + off, s.h_res + off + n);
-      off += (uint32_t)n;
+    {
+      NvtxRange range("myers server: hand back results");
+      for (Request* r : s.reqs) {
+        const size_t n = r->pos.size();
+        r->res.assign(s.h_res + off, s.h_res + off + n);
+        off += (uint32_t)n;
+      }
     }
     lk.lock();
     for (Request* r : s.reqs) {

@@ -620,6 +620,7 @@ extern "C" int myersTraceback(myersTraceback_t* tb, const myersReference_t* ref,
     return MYERS_E_INVALID_ARGUMENT;
   if (numCandidates > tb->capacity) return MYERS_E_CAPACITY;
   if (ref->device != tb->device) return MYERS_E_INVALID_ARGUMENT;
+  NvtxRange range("myers: traceback (select, count, passes)");
   cudaError_t e = cudaSetDevice(tb->device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   cudaStream_t s = (cudaStream_t)stream;

@@ -2,9 +2,10 @@
 against the oracle: the reference-pinned results with the cut-off contract
 applied (oracle.apply_cutoff: a minimum above (uint32_t)(m * cutoff) becomes
 {NO_MATCH, NO_MATCH}; everything else unchanged). Integer outputs: bit-exact.
-The cut-off kernels skip the DP rows above the band, so these tests compare
-their exact scores and first columns wherever the minimum is within the
-bound, including minima equal to it."""
+On the plain path the cut-off settles most candidates from the DP of a
+prefix of their query and runs the rest in full, so these tests compare exact
+scores and first columns wherever the minimum is within the bound, including
+minima equal to it, and the no-match marker everywhere else."""
 import numpy as np
 import pytest
 
@@ -65,9 +66,9 @@ def test_exact_window_cutoff(gpu, orc, data):
 
 
 def test_minimum_at_the_bound(gpu, orc, data):
-    """Bounds placed at the true minima of the candidates of one length (the
-    W = 32 cut-off kernel): a minimum equal to the bound is reported exactly,
-    one above it is not."""
+    """Bounds placed at the true minima of candidates of one length (1,000
+    bases, one candidate per lane of 32 words): a minimum equal to the bound is
+    reported exactly, one above it is not."""
     ref_words, ref_size, ref, ws = data
     w = ws[2]  # 1000-base reads
     full = orc.verify(w["peq"], w["qinfo"], w["cands"], ref_words, ref_size, DIST)
@@ -119,3 +120,38 @@ def test_dropin_buffer_cutoff(gpu, orc, data, tmp_path):
         bufs.set_cutoff(None)
         res, st = gpu.verify_buffers(bufs, w["peq"], w["qinfo"], w["cands"], DIST)
         assert st == gpu.SUCCESS and np.array_equal(res, full)
+
+
+@pytest.mark.parametrize("mult", ["0.25", "1", "100"])
+def test_prefix_multiplier_extremes(mult):
+    """The first pass's prefix length comes from MYERS_CUTOFF_PREFIX (read once
+    per process). A tiny multiplier sends almost every candidate to the second
+    pass; a huge one makes the first pass run every query in full. Both must
+    give the contract's results (a child process per setting)."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import sys, numpy as np
+sys.path.insert(0, "myers-gpu_b200"); sys.path.insert(0, "oracle")
+import myersgpu as mg, oracle as orc
+ref_size = 3_000_000
+rw = mg.make_reference(ref_size, 99)
+ref = mg.Reference(rw, ref_size)
+for k, sc in ((2, 0.002), (3, 0.001), (4, 0.001)):
+    w = mg.make_workload(mg.workload_spec(k, scale=sc, ref_size=ref_size), rw)
+    full = orc.verify(w["peq"], w["qinfo"], w["cands"], rw, ref_size, 0.2)
+    for cutoff in (0.03, 0.1, 0.25):
+        ctx = mg.Context(len(w["cands"]))
+        got = mg.verify_torch(ctx, ref, w["peq"], w["qinfo"], w["cands"], 0.2, cutoff=cutoff)
+        ctx.close()
+        exp = orc.apply_cutoff(full, w["qinfo"], w["cands"], cutoff)
+        assert np.array_equal(got, exp), (k, cutoff, int((got != exp).sum()))
+ref.close()
+print("ok")
+'''
+    from conftest import ROOT
+    env = dict(os.environ, MYERS_CUTOFF_PREFIX=mult)
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stderr[-2000:]
