@@ -531,7 +531,7 @@ def run_ours(args):
         }
         if configs is not None:
             line["configs"] = configs
-            line["north_star"] = north_star_summary(value, configs)
+            line["targets"] = targets_summary(value, configs)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -636,7 +636,7 @@ def run_configs(mg, ms, args, ref3, peak, tmp, threads, padded3):
     return out
 
 
-def north_star_summary(value_plain_1000b, configs):
+def targets_summary(value_plain_1000b, configs):
     """The targets, as measured in this line."""
     sv = configs["serving"]
     records = []  # every per-path record of every configuration

@@ -245,7 +245,7 @@ int myersVerifyRangeAsync(myersContext_t *ctx, const myersReference_t *ref,
  *  - candidates that are not verified (window out of range, invalid indices,
  *    unsupported sizes) get {0, 0xFFFFFFFF} as without the cut-off.
  * On the plain path the work is cut in two passes: the first runs every
- * candidate's DP over a prefix of its query of about 2k rows (the environment
+ * candidate's DP over a prefix of its query of about 2.25k rows (the environment
  * variable MYERS_CUTOFF_PREFIX sets the multiplier), which settles every
  * candidate whose prefix minimum exceeds k (every path to the last row
  * crosses the prefix's last row); the second runs the full DP of the rest.

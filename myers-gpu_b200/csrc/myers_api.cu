@@ -426,7 +426,7 @@ float myers::cutoff_prefix_mult() {
   static const float mult = [] {
     const char* env = getenv("MYERS_CUTOFF_PREFIX");
     const float v = env ? strtof(env, nullptr) : 0.0f;
-    return v > 0.0f ? v : 2.0f;
+    return v > 0.0f ? v : 2.25f;
   }();
   return mult;
 }
@@ -434,7 +434,7 @@ float myers::cutoff_prefix_mult() {
 uint32_t myers::host_prefix_rows(uint32_t m, float cutoff, float mult) {
   const uint32_t k = (uint32_t)((float)m * cutoff);
   const float r = mult * (float)k;
-  const uint32_t rows = r >= 65536.0f ? 0xFFFFFFFFu : (((uint32_t)r + 63u) & ~31u);
+  const uint32_t rows = r >= 65536.0f ? 0xFFFFFFFFu : (((uint32_t)r + 8u + 31u) & ~31u);
   return rows < m ? rows : m;
 }
 

@@ -24,12 +24,12 @@ __device__ __forceinline__ uint32_t d_cutoff_bound(uint32_t m, float cutoff) {
 }
 
 // Rows of the cut-off's first pass for a query of m bases with bound k: k
-// times the multiplier (float32, truncated), plus 32, rounded up to whole
+// times the multiplier (float32, truncated), plus 8, rounded up to whole
 // 32-row words, at most m. The same arithmetic as host_prefix_rows.
 __device__ __forceinline__ uint32_t d_prefix_rows(uint32_t m, float cutoff, float mult) {
   const uint32_t k = d_cutoff_bound(m, cutoff);
   const float r = __fmul_rn(mult, (float)k);
-  const uint32_t rows = r >= 65536.0f ? 0xFFFFFFFFu : (((uint32_t)r + 63u) & ~31u);
+  const uint32_t rows = r >= 65536.0f ? 0xFFFFFFFFu : (((uint32_t)r + 8u + 31u) & ~31u);
   return rows < m ? rows : m;
 }
 

@@ -45,7 +45,11 @@ struct Cand {
 // candidate over L lanes of W words and hand the horizontal delta from lane
 // to lane once per column.
 constexpr int kNumSingle = 32;
+#ifdef MYERS_MORE_WIDTHS
+constexpr int kMultiW[] = {4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 32};
+#else
 constexpr int kMultiW[] = {4, 5, 6, 7, 8, 10, 12, 16, 32};
+#endif
 constexpr int kNumMulti = sizeof(kMultiW) / sizeof(kMultiW[0]);
 constexpr int kNumVariants = kNumSingle + kNumMulti;
 // The persistent kernel carries every single-lane shape and multi-lane
@@ -236,9 +240,10 @@ int cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, fl
 uint32_t host_prefix_rows(uint32_t m, float cutoff, float prefix_mult);
 // Device scratch of the cut-off's second pass for a context (once).
 int ensure_cutoff_scratch(myersContext* ctx);
-// The multiplier of the first pass's rows (MYERS_CUTOFF_PREFIX, default 2:
-// the fastest of 1, 1.5, 2, 2.5, 3 and 4 on 1,000-base reads at bounds of
-// 0.04 to 0.2 of m).
+// The multiplier of the first pass's rows (MYERS_CUTOFF_PREFIX, default
+// 2.25). A random decoy's prefix minimum sits close to 0.46-0.49 per row, so
+// a prefix of 2.25 k rows (plus 8, rounded up to a word) settles almost every
+// decoy while staying short.
 float cutoff_prefix_mult();
 
 // Capture what enqueue() puts on stream s and launch it as the graph *exec.
