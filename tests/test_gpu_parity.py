@@ -106,15 +106,16 @@ def _forced_shape(gpu, orc, workloads, W, L, path):
     assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], w["cands"], ref, ref_size, DIST))
 
 
-@pytest.mark.parametrize("variant_L", [(4, 2), (4, 9), (5, 7), (6, 6), (7, 5), (8, 4), (10, 3), (12, 3), (16, 2),
-                                       (32, 2)])
+@pytest.mark.parametrize("variant_L", [(4, 2), (4, 9), (5, 7), (6, 6), (7, 5), (8, 4), (9, 4), (10, 3), (11, 3),
+                                       (12, 3), (13, 3), (14, 2), (15, 3), (16, 2), (32, 2)])
 def test_every_multi_shape(gpu, orc, workloads, variant_L):
     """Force each multi-lane variant (including L not dividing 32) on reads
     of up to 1000 bases in the plain kernel and compare with the oracle."""
     _forced_shape(gpu, orc, workloads, *variant_L, gpu.PATH_PLAIN)
 
 
-@pytest.mark.parametrize("variant_L", [(4, 8), (5, 7), (6, 6), (7, 5), (8, 4), (10, 4), (12, 3), (16, 2)])
+@pytest.mark.parametrize("variant_L", [(4, 8), (5, 7), (6, 6), (7, 5), (8, 4), (9, 4), (10, 4), (11, 3), (12, 3),
+                                       (13, 3), (14, 3), (15, 2), (16, 2)])
 def test_every_multi_shape_persistent(gpu, orc, workloads, variant_L):
     """The same in the persistent kernel (the serving loop's latency shapes
     run there): every multi-lane width it carries."""
