@@ -27,8 +27,8 @@ JSON line (rank 0).
   configs   (1 GPU, default workload) the other configurations, each with its
             own timing, clocks, roofline fraction and reference parity sample:
             plain-100b, batched-mixed (batched and plain, full size and a
-            110K-candidate batch), batched-long, plain-1000b under Ukkonen's
-            cut-off, and a short serving sweep
+            110K-candidate batch), batched-long, plain-1000b and batched-mixed
+            under Ukkonen's cut-off, and a short serving sweep
 
 --impl reference times the reference's own CPU implementation instead (the
 GPU path of the reference targets sm_20..sm_50 only).
@@ -630,6 +630,15 @@ def run_configs(mg, ms, args, ref3, peak, tmp, threads, padded3):
                                       "cutoff": 0.08, **cut}
     del w2
 
+    # batched-mixed under the cut-off at 0.08 m: the two passes as two
+    # persistent launches
+    _, _, _, w3 = make_inputs(ms, 3, 1.0, 0)
+    cutb, _ = config_record(mg, ms, ref3, w3, mg.PATH_BATCHED, steps, warmup, peak, rw, rs, threads, padded3,
+                            0.02, 306, cutoff=0.08)
+    out["batched-mixed-cutoff-0.08"] = {"workload": WORKLOAD_NAMES[3] + ", Ukkonen's cut-off at 0.08 m",
+                                        "cutoff": 0.08, **cutb}
+    del w3
+
     # serving: a short sweep around the knee
     out["serving"] = serving_sweep(mg, ms, args, ref3, rw, rs, SERVING_RATES_SHORT, steps=min(steps, 5),
                                    warmup=warmup, threads=threads, padded=padded3)
@@ -648,6 +657,8 @@ def targets_summary(value_plain_1000b, configs):
             + [sv["results_equal_to_batched"]])
     return {
         "cutoff_0.08_over_plain_1000b": configs["plain-1000b-cutoff-0.08"]["value"] / value_plain_1000b,
+        "cutoff_0.08_over_batched_mixed": (configs["batched-mixed-cutoff-0.08"]["value"] /
+                                           configs["batched-mixed"]["batched"]["value"]),
         "batched_over_plain_mixed_full": configs["batched-mixed"]["batched_over_plain"],
         "batched_over_plain_mixed_110k": configs["batched-mixed-110k"]["batched_over_plain"],
         "batched_over_plain_long": configs["batched-long"]["batched_over_plain"],

@@ -244,14 +244,14 @@ int myersVerifyRangeAsync(myersContext_t *ctx, const myersReference_t *ref,
  *  - a candidate whose minimum exceeds k gets {MYERS_NO_MATCH, MYERS_NO_MATCH};
  *  - candidates that are not verified (window out of range, invalid indices,
  *    unsupported sizes) get {0, 0xFFFFFFFF} as without the cut-off.
- * On the plain path the work is cut in two passes: the first runs every
+ * The work is cut in two passes: the first runs every
  * candidate's DP over a prefix of its query of about 2.25k rows (the environment
  * variable MYERS_CUTOFF_PREFIX sets the multiplier), which settles every
  * candidate whose prefix minimum exceeds k (every path to the last row
  * crosses the prefix's last row); the second runs the full DP of the rest.
  * The first call on a context allocates the second pass's scratch (5 bytes
- * per candidate of its capacity). The batched path computes every row and
- * applies the same contract. */
+ * per candidate of its capacity). On the batched path the two passes are two
+ * persistent launches. */
 int myersVerifyCutoffAsync(myersContext_t *ctx, const myersReference_t *ref,
                            const qryEntry_t *d_peq, uint32_t numPEQEntries,
                            const qryInfo_t *d_qinfo, uint32_t numQueries,

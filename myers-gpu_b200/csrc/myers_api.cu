@@ -438,7 +438,8 @@ uint32_t myers::host_prefix_rows(uint32_t m, float cutoff, float mult) {
   return rows < m ? rows : m;
 }
 
-int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float mult) {
+int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float mult,
+                        bool batched) {
   uint8_t w1[kMaxWords + 1], w2[kMaxWords + 1];
   memset(w1, 0, sizeof(w1));
   memset(w2, 0, sizeof(w2));
@@ -448,8 +449,8 @@ int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* presen
     w1[(r + 31) / 32] = 1;
     if (r < m) w2[(m + 31) / 32] = 1;
   }
-  const int st = build_plan(plan, w1, false);
-  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, false);
+  const int st = build_plan(plan, w1, batched);
+  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, batched);
 }
 
 extern "C" uint32_t myersContextLastLaunches(const myersContext_t* c) { return c ? c->last_launches : 0; }
@@ -488,6 +489,48 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     const Shape sh = plan.shape[c];
     return launch_plain(sh.variant, sh.L, in, ids, st, (int)c, 0, count, next, s, ctx->num_sms);
   };
+  if (in.cut && path == MYERS_PATH_BATCHED && plan2 != nullptr) {
+    // The cut-off's two passes as two persistent launches: the first over
+    // the prefixes' tiles (plan), then the tile layout of the lists it filled,
+    // then the second over those lists' full queries (plan2). Shapes the
+    // persistent kernel does not carry get plain launches after each.
+    if (ctx->d_esc_ids == nullptr) return MYERS_E_INVALID_ARGUMENT;  // ensure_cutoff_scratch first
+    in.prefix = 1;
+    in.esc_ids = ctx->d_esc_ids;
+    in.esc_state = ctx->d_esc_state;
+    in.esc_cfg = ctx->d_esc_cfg;
+    CU(cudaMemsetAsync(ctx->d_esc_state, 0, sizeof(BucketState), s));
+    CU(cudaMemsetAsync(ctx->d_state, 0, sizeof(BucketState), s));
+    cudaError_t e = cudaSuccess;
+    uint32_t launches = (uint32_t)launch_bucketing_cutoff(in, plan, *plan2, ctx->d_state, ctx->d_cfg, ctx->d_ids, s,
+                                                          ctx->num_sms, &e);
+    if (e != cudaSuccess) return cuda_fail(e, "bucketing");
+    if (plan.num_batched > 0) {
+      CU(launch_batched(in, ctx->d_ids, plan, ctx->d_state, s, ctx->num_sms, batched_tile_bound(plan, in.num_cands)));
+      ++launches;
+    }
+    for (uint32_t c = plan.num_batched; c < plan.num_cfg; ++c) {
+      CU(plain(c, ctx->d_ids, ctx->d_state, 0, &ctx->d_state->next[c]));
+      ++launches;
+    }
+    DevInputs in2 = in;
+    in2.prefix = 0;
+    CU(launch_plan_tiles(*plan2, ctx->d_esc_state, s));
+    ++launches;
+    if (plan2->num_batched > 0) {
+      CU(launch_batched(in2, ctx->d_esc_ids, *plan2, ctx->d_esc_state, s, ctx->num_sms,
+                        batched_tile_bound(*plan2, in.num_cands)));
+      ++launches;
+    }
+    for (uint32_t c = plan2->num_batched; c < plan2->num_cfg; ++c) {
+      const Shape sh = plan2->shape[c];
+      CU(launch_plain(sh.variant, sh.L, in2, ctx->d_esc_ids, ctx->d_esc_state, (int)c, 0, 0,
+                      &ctx->d_esc_state->next[c], s, ctx->num_sms));
+      ++launches;
+    }
+    ctx->last_launches = launches;
+    return MYERS_SUCCESS;
+  }
   if (in.cut && path == MYERS_PATH_PLAIN && plan2 != nullptr) {
     // Ukkonen's cut-off in two passes. The first runs every candidate's DP
     // on a prefix of its query (plan: the prefixes' shapes) and settles the
@@ -618,14 +661,14 @@ static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const 
   if (numCandidates > 0 && (d_peq == nullptr || d_qinfo == nullptr || d_cands == nullptr || d_results == nullptr))
     return MYERS_E_INVALID_ARGUMENT;
   PlanTable plan, plan2;
-  const bool two_pass = cutoff >= 0.0f && path == MYERS_PATH_PLAIN;
+  const bool two_pass = cutoff >= 0.0f;
   const float mult = cutoff_prefix_mult();
   int st;
   if (two_pass) {
     std::vector<uint8_t> present_m(kMaxWords * 32 + 1, 0);
     const uint32_t hi = (maxQuerySize == 0 || maxQuerySize > kMaxWords * 32) ? kMaxWords * 32 : maxQuerySize;
     for (uint32_t m = minQuerySize ? minQuerySize : 1; m <= hi; ++m) present_m[m] = 1;
-    st = cutoff_plans(plan, plan2, present_m.data(), cutoff, mult);
+    st = cutoff_plans(plan, plan2, present_m.data(), cutoff, mult, path == MYERS_PATH_BATCHED);
     if (st == MYERS_SUCCESS) st = ensure_cutoff_scratch(ctx);
   } else {
     st = plan_for_range(plan, minQuerySize, maxQuerySize, path);
@@ -964,7 +1007,7 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
     if (m > 0 && m <= kMaxWords * 32) present[(m + 31) / 32] = 1;  // longer: flagged on the device
   }
   PlanTable& plan = b->plan;
-  const bool two_pass = b->cutoff >= 0.0f && b->path == MYERS_PATH_PLAIN;
+  const bool two_pass = b->cutoff >= 0.0f;
   int st;
   {
     NvtxRange plan_range("myers: send: shape plan");
@@ -975,7 +1018,7 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
         const uint32_t m = b->h_qinfo[q].size;
         if (m > 0 && m <= kMaxWords * 32) pm[m] = 1;
       }
-      st = cutoff_plans(plan, b->plan2, pm.data(), b->cutoff, cutoff_prefix_mult());
+      st = cutoff_plans(plan, b->plan2, pm.data(), b->cutoff, cutoff_prefix_mult(), b->path == MYERS_PATH_BATCHED);
     } else {
       st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
     }

@@ -165,6 +165,10 @@ int launch_bucketing_cutoff(const DevInputs& in, const PlanTable& plan, const Pl
                             BucketState* d_state, uint8_t* d_cfg_of_cand, uint32_t* d_ids, cudaStream_t s,
                             int num_sms, cudaError_t* err);
 
+// The cut-off's second pass on the persistent path: tile layout of the lists
+// the first pass filled (d_esc_state), after the first pass.
+cudaError_t launch_plan_tiles(const PlanTable& plan2, BucketState* d_esc_state, cudaStream_t s);
+
 // The persistent batched launch over the plan's first num_batched shapes;
 // the grid is the device's resident capacity or, for small batches, one
 // warp per tile of `max_tiles` (an upper bound of the tiles), whichever is
@@ -227,15 +231,16 @@ struct myersContext {
 
 namespace myers {
 // Enqueue the kernels of one batch on stream s (inputs already on the device).
-// With in.cut on the plain path the cut-off runs in two passes: `plan` must
-// then hold the first pass's (prefix) shapes and `plan2` the full-length
-// shapes (cutoff_plans).
+// With in.cut and plan2 given, the cut-off runs in two passes: `plan` holds
+// the first pass's (prefix) shapes and `plan2` the full-length shapes
+// (cutoff_plans), on either path.
 int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs& in, const PlanTable& plan, int path,
                    cudaStream_t s, const PlanTable* plan2 = nullptr);
 // The cut-off's plans from the word counts of the full queries present: the
 // first pass's prefix shapes into `plan`, the full-length shapes into
 // `plan2`. `present_m[m]` flags each query length m (1..kMaxWords*32).
-int cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float prefix_mult);
+int cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float prefix_mult,
+                 bool batched);
 // The first pass's rows of a query of m bases (as prefix_rows on the device).
 uint32_t host_prefix_rows(uint32_t m, float cutoff, float prefix_mult);
 // Device scratch of the cut-off's second pass for a context (once).

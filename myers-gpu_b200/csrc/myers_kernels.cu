@@ -700,6 +700,24 @@ __global__ void k_plan_escalation(const __grid_constant__ PlanTable plan2, Bucke
   }
 }
 
+// The second pass's tiles on the persistent path, once the first pass has
+// filled the lists: each shape's tiles from its list length, the persistent
+// kernel's tile count and a fresh work counter.
+__global__ void k_plan_tiles(const __grid_constant__ PlanTable plan2, BucketState* esc) {
+  if (threadIdx.x != 0) return;
+  uint32_t tiles = 0;
+  for (uint32_t c = 0; c < plan2.num_cfg; ++c) {
+    const Shape s = plan2.shape[c];
+    const uint32_t nseg = (s.variant >= kNumSingle) ? 32u / s.L : 32u;
+    if (c == plan2.num_batched) esc->total_tiles = tiles;
+    esc->tile_start[c] = tiles;
+    tiles += (esc->count[c] + nseg - 1) / nseg;
+  }
+  esc->tile_start[plan2.num_cfg] = tiles;
+  if (plan2.num_batched >= plan2.num_cfg) esc->total_tiles = tiles;
+  esc->queue = 0;
+}
+
 __global__ void k_plan(const __grid_constant__ PlanTable plan, BucketState* st) {
   if (threadIdx.x != 0) return;
   uint32_t acc = 0, tiles = 0;
@@ -916,6 +934,11 @@ int launch_bucketing_cutoff(const DevInputs& in, const PlanTable& plan, const Pl
   k_scatter<<<grid, threads, 0, s>>>(in.num_cands, d_cfg_of_cand, d_state, d_ids);
   *err = cudaGetLastError();
   return 4;
+}
+
+cudaError_t launch_plan_tiles(const PlanTable& plan2, BucketState* d_esc_state, cudaStream_t s) {
+  k_plan_tiles<<<1, 32, 0, s>>>(plan2, d_esc_state);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_batched(const DevInputs& in, const uint32_t* d_ids, const PlanTable& plan,

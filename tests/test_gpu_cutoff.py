@@ -142,11 +142,12 @@ for k, sc in ((2, 0.002), (3, 0.001), (4, 0.001)):
     w = mg.make_workload(mg.workload_spec(k, scale=sc, ref_size=ref_size), rw)
     full = orc.verify(w["peq"], w["qinfo"], w["cands"], rw, ref_size, 0.2)
     for cutoff in (0.03, 0.1, 0.25):
-        ctx = mg.Context(len(w["cands"]))
-        got = mg.verify_torch(ctx, ref, w["peq"], w["qinfo"], w["cands"], 0.2, cutoff=cutoff)
-        ctx.close()
         exp = orc.apply_cutoff(full, w["qinfo"], w["cands"], cutoff)
-        assert np.array_equal(got, exp), (k, cutoff, int((got != exp).sum()))
+        for path in (mg.PATH_PLAIN, mg.PATH_BATCHED):
+            ctx = mg.Context(len(w["cands"]))
+            got = mg.verify_torch(ctx, ref, w["peq"], w["qinfo"], w["cands"], 0.2, cutoff=cutoff, path=path)
+            ctx.close()
+            assert np.array_equal(got, exp), (k, cutoff, path, int((got != exp).sum()))
 ref.close()
 print("ok")
 '''
