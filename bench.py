@@ -493,7 +493,7 @@ def run_ours(args):
     threads = host_threads()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    padded = orc.pad_reference(ref_words) if orc.have_reference() else None
+    padded = orc.pad_reference(ref_words) if orc.have_reference() and world == 1 and not args.no_cpu else None
     if world == 1 and not args.no_cpu:
         parity, cpu = reference_parity(w, res, ref_words, ref_size, args.parity_frac, 11, threads, padded,
                                        args.cutoff)
