@@ -7,16 +7,19 @@ for each multi-lane width W (the persistent kernel carries W <= 16). For every
 bucket 1..32 and a sample of longer ones, each shape is timed on a seeded
 workload of reads of 32*w bases, about 1e13 cells (20K..4M candidates) so
 that every shape runs many waves (CUDA events, best of three after a warm-up);
-the fastest wins. On the plain path, unsampled long buckets take the width
-of the nearest sampled bucket above them, with L = ceil(w/W). On the batched
-path, every bucket of 33..512 words takes the multi-lane shape that the cost
-model ranks first (model_shape): with a width for every lane count from 4 to
-16 words the model's choice, which counts idle lanes and padding rows,
-measured 5% faster on reads of 1,000..10,000 bases than the nearest-sample
-fill.
+the fastest wins. Unsampled long buckets take the width of the nearest
+sampled bucket above them, with L = ceil(w/W).
+
+The batched path has a second table for large batches ("batched_large", used
+from 150K candidates on): every bucket of 33..512 words takes the multi-lane
+shape that the cost model ranks first (model_shape), over every width from 4
+to 16 words. The model counts idle lanes and padding rows, and on 500K
+long-read candidates its shapes ran 5% faster than the sampled ones. In small
+batches the many shapes they use run side by side in the persistent kernel
+and thrash its instruction cache, so small batches keep the sampled table.
 
     python myers-gpu_b200/autotune.py [--out PATH] [--quick]
-    python myers-gpu_b200/autotune.py --refill-batched-long   # no GPU: redo that fill in the cache
+    python myers-gpu_b200/autotune.py --refill-batched-long   # no GPU: rewrite batched_large in the cache
 
 writes autotune_b200.json next to the library (the runtime loads it at
 start); the file also keeps every measurement.
@@ -72,7 +75,8 @@ BATCHED_MODEL_WORDS = range(33, 513)  # buckets the persistent kernel's widths (
 
 
 def refill_batched_long(table, widths):
-    """The batched path's buckets of 33..512 words by model_shape."""
+    """The large-batch table of the batched path: buckets of 33..512 words by
+    model_shape."""
     for w in BATCHED_MODEL_WORDS:
         shape = model_shape(w, [W for W in widths if W <= 16])
         if shape:
@@ -92,10 +96,11 @@ def main():
         widths = sorted(W for _, W, multi in mg.variants() if multi)
         with open(args.out) as f:
             cache = json.load(f)
-        refill_batched_long(cache["batched"], widths)
-        cache["method"] = cache["method"].split("; batched 33..512")[0] + \
-            "; batched 33..512 words: the cost model over multi-lane widths " + \
-            ",".join(str(W) for W in widths if W <= 16)
+        cache["batched_large"] = {}
+        refill_batched_long(cache["batched_large"], widths)
+        cache["method"] = cache["method"].split("; batched")[0] + \
+            "; batched_large (batches of 150K candidates or more), 33..512 words: the cost model over " + \
+            "multi-lane widths " + ",".join(str(W) for W in widths if W <= 16)
         with open(args.out, "w") as f:
             json.dump(cache, f)
         print("rewrote", args.out)
@@ -154,14 +159,12 @@ def main():
         print(f"w={w:5d} m={m:6d} n={n:8d} plain={measured['plain'][w]['shape']} "
               f"batched={measured['batched'][w]['shape']} ({time.time() - t_start:.0f}s)", flush=True)
 
-    table = {"plain": {}, "batched": {}}
+    table = {"plain": {}, "batched": {}, "batched_large": {}}
     widths = {W: v for v, W, multi in mg.variants() if multi}
-    refill_batched_long(table["batched"], sorted(widths))
+    refill_batched_long(table["batched_large"], sorted(widths))
     for pname in ("plain", "batched"):
         sampled = sorted(measured[pname])
         for w in range(1, 1025):
-            if pname == "batched" and w in BATCHED_MODEL_WORDS:
-                continue  # the cost model's shape (refill_batched_long)
             if w in measured[pname]:
                 v, L, W = measured[pname][w]["shape"]
                 table[pname][w] = [W, L]
@@ -187,6 +190,7 @@ def main():
            "format": "plain/batched: words -> [W words per lane, L lanes per candidate]",
            "plain": {str(k): v for k, v in table["plain"].items()},
            "batched": {str(k): v for k, v in table["batched"].items()},
+           "batched_large": table["batched_large"],
            "measured": {p: {str(k): v for k, v in measured[p].items()} for p in measured}}
     with open(args.out, "w") as f:
         json.dump(out, f)

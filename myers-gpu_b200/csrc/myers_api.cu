@@ -189,13 +189,15 @@ struct Override {
 };
 static std::mutex g_override_mu;
 static Override g_override[2][kMaxWords + 1];
-static Override g_tuned[2][kMaxWords + 1];  // from the autotuner's cache file
+// from the autotuner's cache file: plain, batched, and batched for large
+// batches (see large_batch)
+static Override g_tuned[3][kMaxWords + 1];
 
 // Load the autotuner's cache: `autotune_b200.json` next to this library (or
 // the file named by MYERS_AUTOTUNE; MYERS_AUTOTUNE=0 disables it). Format:
-// {"plain": {"<words>": [W, L], ...}, "batched": {...}, ...} with W words per
-// lane and L lanes per candidate; entries naming a shape that is not compiled
-// or that the path cannot run are ignored.
+// {"plain": {"<words>": [W, L], ...}, "batched": {...}, "batched_large": {...}}
+// with W words per lane and L lanes per candidate; entries naming a shape that
+// is not compiled or that the path cannot run are ignored.
 static void load_tuned_once() {
   static std::once_flag once;
   std::call_once(once, [] {
@@ -219,8 +221,8 @@ static void load_tuned_once() {
     while ((n = fread(buf, 1, sizeof(buf), fp)) > 0) text.append(buf, n);
     fclose(fp);
     std::lock_guard<std::mutex> lk(g_override_mu);
-    for (int path_id = 0; path_id < 2; ++path_id) {
-      const char* key = path_id == 0 ? "\"plain\"" : "\"batched\"";
+    for (int path_id = 0; path_id < 3; ++path_id) {
+      const char* key = path_id == 0 ? "\"plain\"" : path_id == 1 ? "\"batched\"" : "\"batched_large\"";
       size_t at = text.find(key);
       if (at == std::string::npos) continue;
       at = text.find('{', at);
@@ -250,11 +252,27 @@ static void load_tuned_once() {
   });
 }
 
+// Whether a batch of n candidates takes the batched path's shapes for large
+// batches. Those use every lane width, which fills the lanes best; but the
+// persistent kernel runs whatever tiles come next, and in a small batch of
+// long reads the tiles of many different shapes run side by side and thrash
+// the instruction cache (10K long-read candidates: 12.2 ms with them, 8.2 ms
+// with the few-width table; 125K: 80.1 against 79.2 ms; 250K: 151.3 against
+// 156.6 ms; 500K: 296 against 312 ms). MYERS_LARGE_BATCH sets the threshold
+// in candidates.
+static bool large_batch(uint64_t n) {
+  static const uint64_t threshold = [] {
+    const char* env = getenv("MYERS_LARGE_BATCH");
+    return env ? strtoull(env, nullptr, 10) : (uint64_t)kLargeBatchCandidates;
+  }();
+  return n >= threshold;
+}
+
 // lane_words > 0 asks for latency-oriented shapes: a query of more than
 // lane_words words is spread over ceil(words / W) lanes of W <= lane_words
 // words, the cheapest such shape by the cost model (shorter per-candidate
-// time, some more instructions).
-static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
+// time, some more instructions). `large`: the batch is large (large_batch).
+static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0, bool large = false) {
   load_tuned_once();
   {
     std::lock_guard<std::mutex> lk(g_override_mu);
@@ -281,6 +299,10 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
   }
   {
     std::lock_guard<std::mutex> lk(g_override_mu);
+    if (batched && large && g_tuned[2][w].set) {
+      const Override& o = g_tuned[2][w];
+      return Shape{o.variant, o.L, (uint8_t)variant_W(o.variant), 0};
+    }
     const Override& o = g_tuned[batched ? 1 : 0][w];
     if (o.set) return Shape{o.variant, o.L, (uint8_t)variant_W(o.variant), 0};
   }
@@ -304,7 +326,7 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0) {
 
 // Build the plan for the word counts flagged in `present` (size kMaxWords+1).
 // Uses fixed-size stack arrays only: no allocation on the send path.
-int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words) {
+int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words, uint64_t n) {
   memset(&t, 0, sizeof(t));
   memset(t.cfg_of_words, kNoCfg, sizeof(t.cfg_of_words));
   Shape shapes[kMaxCfg];
@@ -314,7 +336,7 @@ int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32
   for (uint32_t w = 0; w <= kMaxWords; ++w) cfg_of[w] = -1;
   for (uint32_t w = 1; w <= kMaxWords; ++w) {
     if (!present[w]) continue;
-    const Shape s = pick_shape(w, batched, lane_words);
+    const Shape s = pick_shape(w, batched, lane_words, large_batch(n));
     if (s.L == 0) return MYERS_E_QUERY_TOO_LONG;
     int found = -1;
     for (int i = 0; i < nshapes; ++i)
@@ -439,7 +461,7 @@ uint32_t myers::host_prefix_rows(uint32_t m, float cutoff, float mult) {
 }
 
 int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float mult,
-                        bool batched) {
+                        bool batched, uint64_t n) {
   uint8_t w1[kMaxWords + 1], w2[kMaxWords + 1];
   memset(w1, 0, sizeof(w1));
   memset(w2, 0, sizeof(w2));
@@ -449,8 +471,8 @@ int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* presen
     w1[(r + 31) / 32] = 1;
     if (r < m) w2[(m + 31) / 32] = 1;
   }
-  const int st = build_plan(plan, w1, batched);
-  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, batched);
+  const int st = build_plan(plan, w1, batched, 0, n);
+  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, batched, 0, n);
 }
 
 extern "C" uint32_t myersContextLastLaunches(const myersContext_t* c) { return c ? c->last_launches : 0; }
@@ -599,14 +621,14 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
   return MYERS_SUCCESS;
 }
 
-static int plan_for_range(PlanTable& plan, uint32_t minSize, uint32_t maxSize, int path) {
+static int plan_for_range(PlanTable& plan, uint32_t minSize, uint32_t maxSize, int path, uint64_t n) {
   uint8_t present[kMaxWords + 1];
   memset(present, 0, sizeof(present));
   if (maxSize == 0) maxSize = kMaxWords * 32;
   if (maxSize > kMaxWords * 32) maxSize = kMaxWords * 32;
   const uint32_t wlo = minSize ? (minSize + 31) / 32 : 1, whi = (maxSize + 31) / 32;
   for (uint32_t w = wlo; w <= whi; ++w) present[w] = 1;
-  return build_plan(plan, present, path == MYERS_PATH_BATCHED);
+  return build_plan(plan, present, path == MYERS_PATH_BATCHED, 0, n);
 }
 
 extern "C" int myersVerifyAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
@@ -668,10 +690,10 @@ static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const 
     std::vector<uint8_t> present_m(kMaxWords * 32 + 1, 0);
     const uint32_t hi = (maxQuerySize == 0 || maxQuerySize > kMaxWords * 32) ? kMaxWords * 32 : maxQuerySize;
     for (uint32_t m = minQuerySize ? minQuerySize : 1; m <= hi; ++m) present_m[m] = 1;
-    st = cutoff_plans(plan, plan2, present_m.data(), cutoff, mult, path == MYERS_PATH_BATCHED);
+    st = cutoff_plans(plan, plan2, present_m.data(), cutoff, mult, path == MYERS_PATH_BATCHED, numCandidates);
     if (st == MYERS_SUCCESS) st = ensure_cutoff_scratch(ctx);
   } else {
-    st = plan_for_range(plan, minQuerySize, maxQuerySize, path);
+    st = plan_for_range(plan, minQuerySize, maxQuerySize, path, numCandidates);
   }
   if (st != MYERS_SUCCESS) return st;
   DevInputs in;
@@ -1018,9 +1040,10 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
         const uint32_t m = b->h_qinfo[q].size;
         if (m > 0 && m <= kMaxWords * 32) pm[m] = 1;
       }
-      st = cutoff_plans(plan, b->plan2, pm.data(), b->cutoff, cutoff_prefix_mult(), b->path == MYERS_PATH_BATCHED);
+      st = cutoff_plans(plan, b->plan2, pm.data(), b->cutoff, cutoff_prefix_mult(), b->path == MYERS_PATH_BATCHED,
+                        numCandidates);
     } else {
-      st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED);
+      st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED, 0, numCandidates);
     }
   }
   if (st != MYERS_SUCCESS) return b->last_status = st;
@@ -1244,7 +1267,7 @@ extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refW
   int st = noalloc_setup(&dev);
   if (st != MYERS_SUCCESS) return st;
   PlanTable plan;
-  st = plan_for_range(plan, minQuerySize, maxQuerySize, MYERS_PATH_BATCHED);
+  st = plan_for_range(plan, minQuerySize, maxQuerySize, MYERS_PATH_BATCHED, numCandidates);
   if (st != MYERS_SUCCESS) return st;
   BucketState* d_state = reinterpret_cast<BucketState*>(dev.scratch);
   uint32_t* d_ids = reinterpret_cast<uint32_t*>(dev.scratch + kNoAllocIdsOffset);

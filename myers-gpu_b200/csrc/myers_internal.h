@@ -67,6 +67,9 @@ struct Shape {
 };
 
 constexpr int kMaxCfg = 128;            // distinct shapes in one plan
+// Batches of at least this many candidates take the batched path's shapes for
+// large batches (every lane width; the autotuner cache's "batched_large").
+constexpr uint64_t kLargeBatchCandidates = 150000;
 constexpr uint8_t kNoCfg = 0xFF;
 
 // Per-send plan, passed by value as a __grid_constant__ kernel parameter:
@@ -198,7 +201,9 @@ cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iter
 // ---- host runtime internals (myers_api.cu) ----
 
 // Shape plan for the word counts flagged in present[0..kMaxWords].
-int build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words = 0);
+// n: the batch's candidates, which picks the batched path's table for large
+// batches at kLargeBatchCandidates or more.
+int build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words = 0, uint64_t n = 0);
 // Upper bound of the persistent kernel's tiles for n candidates under `plan`.
 uint32_t batched_tile_bound(const PlanTable& plan, uint32_t n);
 // Record a CUDA failure (message for myersGetErrorString) and return MYERS_E_CUDA.
@@ -240,7 +245,7 @@ int verify_enqueue(myersContext* ctx, const myersReference* ref, const DevInputs
 // first pass's prefix shapes into `plan`, the full-length shapes into
 // `plan2`. `present_m[m]` flags each query length m (1..kMaxWords*32).
 int cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* present_m, float cutoff, float prefix_mult,
-                 bool batched);
+                 bool batched, uint64_t n);
 // The first pass's rows of a query of m bases (as prefix_rows on the device).
 uint32_t host_prefix_rows(uint32_t m, float cutoff, float prefix_mult);
 // Device scratch of the cut-off's second pass for a context (once).

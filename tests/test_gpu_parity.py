@@ -321,3 +321,35 @@ def test_concurrent_contexts_on_two_streams(gpu, orc, workloads):
         for j in jobs:
             j["ctx"].close()
         ref.close()
+
+
+def test_large_batch_shapes():
+    """Batches of 150K candidates or more take the batched path's
+    large-batch shapes (every lane width). MYERS_LARGE_BATCH=1 (read once per
+    process, so in a child) gives them to small batches of long and mixed
+    reads, compared with the oracle on both paths."""
+    import subprocess
+    import sys
+    from conftest import ROOT
+    code = r'''
+import sys, numpy as np
+sys.path.insert(0, "myers-gpu_b200"); sys.path.insert(0, "oracle")
+import myersgpu as mg, oracle as orc
+ref_size = 4_000_000
+rw = mg.make_reference(ref_size, 31)
+ref = mg.Reference(rw, ref_size)
+for k, sc in ((4, 0.003), (3, 0.001)):
+    w = mg.make_workload(mg.workload_spec(k, scale=sc, ref_size=ref_size), rw)
+    expect = orc.verify(w["peq"], w["qinfo"], w["cands"], rw, ref_size, 0.2)
+    for path in (mg.PATH_BATCHED, mg.PATH_PLAIN):
+        ctx = mg.Context(len(w["cands"]))
+        got = mg.verify_torch(ctx, ref, w["peq"], w["qinfo"], w["cands"], 0.2, path=path)
+        ctx.close()
+        assert np.array_equal(got, expect), (k, path, int((got != expect).sum()))
+ref.close()
+print("ok")
+'''
+    env = dict(os.environ, MYERS_LARGE_BATCH="1")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0 and "ok" in out.stdout, out.stderr[-2000:]
