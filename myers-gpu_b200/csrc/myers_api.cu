@@ -268,6 +268,22 @@ static bool large_batch(uint64_t n) {
   return n >= threshold;
 }
 
+// Whether a batch of n candidates on the batched path takes latency shapes
+// (lanes of at most kSmallBatchLaneWords words) for reads of up to 1,024
+// bases. A small batch runs about one wave of tiles and ends with its longest
+// tile; lanes of 12 words make the tiles of 1,000-base reads a quarter as long
+// for about 13% more instructions (mixed reads of 100..1,000 bases: 11K
+// candidates 0.93 -> 0.45 ms, 110K 1.50 -> 0.90 ms, 220K 1.86 -> 1.70 ms;
+// 330K 2.44 -> 2.53 ms, 1.1M 7.3 -> 8.4 ms).
+// MYERS_SMALL_BATCH sets the threshold in candidates (0 turns it off).
+static bool small_batch(uint64_t n) {
+  static const uint64_t threshold = [] {
+    const char* env = getenv("MYERS_SMALL_BATCH");
+    return env ? strtoull(env, nullptr, 10) : (uint64_t)kSmallBatchCandidates;
+  }();
+  return n > 0 && n < threshold;
+}
+
 // lane_words > 0 asks for latency-oriented shapes: a query of more than
 // lane_words words is spread over ceil(words / W) lanes of W <= lane_words
 // words, the cheapest such shape by the cost model (shorter per-candidate
@@ -334,9 +350,11 @@ int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32
   int16_t cfg_of[kMaxWords + 1];
   int nshapes = 0;
   for (uint32_t w = 0; w <= kMaxWords; ++w) cfg_of[w] = -1;
+  const bool small = batched && lane_words == 0 && small_batch(n);
   for (uint32_t w = 1; w <= kMaxWords; ++w) {
     if (!present[w]) continue;
-    const Shape s = pick_shape(w, batched, lane_words, large_batch(n));
+    const uint32_t lw = (small && w <= 32) ? kSmallBatchLaneWords : lane_words;
+    const Shape s = pick_shape(w, batched, lw, large_batch(n));
     if (s.L == 0) return MYERS_E_QUERY_TOO_LONG;
     int found = -1;
     for (int i = 0; i < nshapes; ++i)

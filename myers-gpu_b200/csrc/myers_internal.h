@@ -70,6 +70,10 @@ constexpr int kMaxCfg = 128;            // distinct shapes in one plan
 // Batches of at least this many candidates take the batched path's shapes for
 // large batches (every lane width; the autotuner cache's "batched_large").
 constexpr uint64_t kLargeBatchCandidates = 150000;
+// Batches below this many candidates take latency shapes on the batched path
+// for reads of up to 1,024 bases: lanes of at most kSmallBatchLaneWords words.
+constexpr uint64_t kSmallBatchCandidates = 280000;
+constexpr uint32_t kSmallBatchLaneWords = 12;
 constexpr uint8_t kNoCfg = 0xFF;
 
 // Per-send plan, passed by value as a __grid_constant__ kernel parameter:

@@ -323,11 +323,17 @@ def test_concurrent_contexts_on_two_streams(gpu, orc, workloads):
         ref.close()
 
 
-def test_large_batch_shapes():
-    """Batches of 150K candidates or more take the batched path's
-    large-batch shapes (every lane width). MYERS_LARGE_BATCH=1 (read once per
-    process, so in a child) gives them to small batches of long and mixed
-    reads, compared with the oracle on both paths."""
+@pytest.mark.parametrize("env", [{"MYERS_LARGE_BATCH": "1", "MYERS_SMALL_BATCH": "0"},
+                                 {"MYERS_SMALL_BATCH": "0"}], ids=["large", "tuned"])
+def test_batch_size_shapes(env):
+    """The batched path picks its shapes by batch size. Below 280K candidates
+    reads of up to 1,024 bases take lanes of at most 12 words (what the other
+    tests' small batches run). Longer reads, and every read from 280K, take the
+    large-batch table (every lane width) from 150K candidates and the tuned
+    table below that. The thresholds (MYERS_SMALL_BATCH,
+    MYERS_LARGE_BATCH, read once per process, so in a child) are moved here so
+    small batches of long and mixed reads run the large-batch and the tuned
+    tables, compared with the oracle on both paths."""
     import subprocess
     import sys
     from conftest import ROOT
@@ -349,7 +355,7 @@ for k, sc in ((4, 0.003), (3, 0.001)):
 ref.close()
 print("ok")
 '''
-    env = dict(os.environ, MYERS_LARGE_BATCH="1")
-    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True,
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=dict(os.environ, **env),
+                         capture_output=True, text=True,
                          timeout=600)
     assert out.returncode == 0 and "ok" in out.stdout, out.stderr[-2000:]
