@@ -372,6 +372,17 @@ struct TbCol {
   uint32_t x;
 };
 
+// Columns the walk fetches ahead of the one it is in.
+#ifndef MYERS_TB_AHEAD
+#define MYERS_TB_AHEAD 4
+#endif
+// The walk's band loads: 0 through L2 only (ld.global.cg); 1 through the
+// read-only path, cached in L1 as well (the bands are written by the forward
+// pass, an earlier kernel).
+#ifndef MYERS_TB_LDG
+#define MYERS_TB_LDG 0
+#endif
+
 __device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const TbGeom& g, uint32_t j1, uint32_t x) {
   TbCol c;
   c.v = make_uint4(0u, 0u, 0u, 0u);
@@ -379,7 +390,11 @@ __device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const 
   if (j1 >= 1u && j1 >= g.a0 && j1 <= g.c1) {
     const uint32_t xa = tb_xlo(g, j1);
     if (x >= xa && x < xa + g.B) {
+#if MYERS_TB_LDG
+      c.v = __ldg(slot + (size_t)(j1 - g.a0) * g.B + (x - xa));
+#else
       c.v = __ldcg(slot + (size_t)(j1 - g.a0) * g.B + (x - xa));
+#endif
       c.x = x;
     }
   }
@@ -398,9 +413,10 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
   uint32_t i = g.m, j1 = g.c1;
   uint32_t nruns = 0, cur = 0, len = 0;
   bool bad = false;
-  // c0: column j1; c1..c4: columns j1-1 .. j1-4 (fetched ahead); all at word xw
+  // cw[0]: column j1; cw[d]: column j1-d (fetched ahead); all at word xw
+  constexpr int D = MYERS_TB_AHEAD;
   uint32_t xw = 0xFFFFFFFFu;
-  TbCol c0, c1, c2, c3, c4;
+  TbCol cw[D + 1];
   // PEQ words of query word qw (five bases); text word twi
   uint32_t qw = 0xFFFFFFFFu, q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
   unsigned long long twi = ~0ull;
@@ -415,14 +431,11 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
       const uint32_t bit = g.p + i - 1u, x = bit >> 5, sh = bit & 31u;
       if (x != xw) {
         xw = x;
-        c0 = tb_fetch(slot, g, j1, x);
-        c1 = tb_fetch(slot, g, j1 - 1u, x);
-        c2 = tb_fetch(slot, g, j1 - 2u, x);
-        c3 = tb_fetch(slot, g, j1 - 3u, x);
-        c4 = tb_fetch(slot, g, j1 - 4u, x);
+#pragma unroll
+        for (int d = 0; d <= D; ++d) cw[d] = tb_fetch(slot, g, j1 - (uint32_t)d, x);
       }
-      if (c0.x != x) c0 = tb_fetch(slot, g, j1, x);
-      if (c0.x != x) {  // the path left the stored band: the data is inconsistent
+      if (cw[0].x != x) cw[0] = tb_fetch(slot, g, j1, x);
+      if (cw[0].x != x) {  // the path left the stored band: the data is inconsistent
         bad = true;
         break;
       }
@@ -443,15 +456,15 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
       const uint32_t code = (twv >> (4u * (uint32_t)(b & 7u))) & 0xFu;
       const uint32_t pq = code == 0 ? q0 : code == 1 ? q1 : code == 2 ? q2 : code == 3 ? q3 : q4;
       const uint32_t match = (pq >> (q & 31u)) & 1u;
-      const int h = tb_delta(c0.v.z, c0.v.w, sh), v = tb_delta(c0.v.x, c0.v.y, sh);
+      const int h = tb_delta(cw[0].v.z, cw[0].v.w, sh), v = tb_delta(cw[0].v.x, cw[0].v.y, sh);
       int vl = 1;  // column 0: D[i][0] = i
       if (j1 - 1u > 0u) {
-        if (c1.x != x) c1 = tb_fetch(slot, g, j1 - 1u, x);
-        if (c1.x != x) {
+        if (cw[1].x != x) cw[1] = tb_fetch(slot, g, j1 - 1u, x);
+        if (cw[1].x != x) {
           bad = true;
           break;
         }
-        vl = tb_delta(c1.v.x, c1.v.y, sh);
+        vl = tb_delta(cw[1].v.x, cw[1].v.y, sh);
       }
       if (h + vl == (int)(1u - match)) {
         op = match ? kOpEq : kOpX;
@@ -465,11 +478,9 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
         --j1;
       }
       if (op != kOpI) {  // one column to the left: shift the window, fetch one more
-        c0 = c1;
-        c1 = c2;
-        c2 = c3;
-        c3 = c4;
-        c4 = tb_fetch(slot, g, j1 >= 4u ? j1 - 4u : 0u, xw);
+#pragma unroll
+        for (int d = 0; d < D; ++d) cw[d] = cw[d + 1];
+        cw[D] = tb_fetch(slot, g, j1 >= (uint32_t)D ? j1 - (uint32_t)D : 0u, xw);
       }
     }
     if (len && op == cur) {
