@@ -47,6 +47,17 @@ static constexpr uint32_t kTbNotTraced = 0xFFFFFFFFu;
 static constexpr uint32_t kTbInconsistent = 0xFFFFFFFEu;
 static constexpr uint32_t kOpEq = 7, kOpX = 8, kOpI = 1, kOpD = 2;  // SAM codes
 
+// Columns the walk fetches ahead of the one it is in.
+#ifndef MYERS_TB_AHEAD
+#define MYERS_TB_AHEAD 4
+#endif
+// The walk's band loads: 0 through L2 only (ld.global.cg); 1 through the
+// read-only path, cached in L1 as well (the bands are written by the forward
+// pass, an earlier kernel).
+#ifndef MYERS_TB_LDG
+#define MYERS_TB_LDG 0
+#endif
+
 // packed = traced count << 36 | their band stores in 256-byte units
 static constexpr unsigned kTbUnitShift = 8;
 static constexpr unsigned kTbCountShift = 36;
@@ -372,16 +383,6 @@ struct TbCol {
   uint32_t x;
 };
 
-// Columns the walk fetches ahead of the one it is in.
-#ifndef MYERS_TB_AHEAD
-#define MYERS_TB_AHEAD 4
-#endif
-// The walk's band loads: 0 through L2 only (ld.global.cg); 1 through the
-// read-only path, cached in L1 as well (the bands are written by the forward
-// pass, an earlier kernel).
-#ifndef MYERS_TB_LDG
-#define MYERS_TB_LDG 0
-#endif
 
 __device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const TbGeom& g, uint32_t j1, uint32_t x) {
   TbCol c;
@@ -390,10 +391,11 @@ __device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const 
   if (j1 >= 1u && j1 >= g.a0 && j1 <= g.c1) {
     const uint32_t xa = tb_xlo(g, j1);
     if (x >= xa && x < xa + g.B) {
+      const uint4* e = slot + (size_t)(j1 - g.a0) * g.B + (x - xa);
 #if MYERS_TB_LDG
-      c.v = __ldg(slot + (size_t)(j1 - g.a0) * g.B + (x - xa));
+      c.v = __ldg(e);
 #else
-      c.v = __ldcg(slot + (size_t)(j1 - g.a0) * g.B + (x - xa));
+      c.v = __ldcg(e);
 #endif
       c.x = x;
     }
