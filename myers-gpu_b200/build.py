@@ -34,20 +34,36 @@ def _run(cmd):
 
 
 def build_cuda(verbose_ptxas=False):
+    """Compile each CUDA source to an object in parallel (the kernels' file
+    takes most of the time), then link the shared library."""
     out = os.path.join(HERE, "libmyers_b200.so")
     srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [__file__]
-    extra =os.environ.get("MYERS_NVCC_FLAGS", "").split()  # e.g. -DMYERS_SHIFT_MODE=2
+    headers = [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [__file__]
+    extra = os.environ.get("MYERS_NVCC_FLAGS", "").split()  # e.g. -DMYERS_SHIFT_MODE=2
     stamp = out + ".flags"
     if os.path.exists(stamp) and open(stamp).read() != " ".join(extra):
         os.remove(out)  # rebuild when the build options change
-    if not _newer(out, deps) and not verbose_ptxas:
+        os.remove(stamp)
+    if not _newer(out, srcs + headers) and not verbose_ptxas:
         return out
-    cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-shared", *extra,
-           "-I", os.path.join(ROOT, "include"), "-o", out, *srcs]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", *extra,
+              "-I", os.path.join(ROOT, "include")]
     if verbose_ptxas:
-        cmd.insert(1, "-Xptxas=-v")
-    _run(cmd)
+        common.insert(1, "-Xptxas=-v")
+    objs, procs = [], []
+    for src in srcs:
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
+        objs.append(obj)
+        if verbose_ptxas or not os.path.exists(stamp) or _newer(obj, [src, stamp] + headers):
+            cmd = common + ["-c", "-o", obj, src]
+            print(" ".join(cmd), flush=True)
+            procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    _run([NVCC, *ARCH, "-shared", "-o", out, *objs])
     with open(stamp, "w") as f:
         f.write(" ".join(extra))
     return out
