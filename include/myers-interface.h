@@ -410,10 +410,12 @@ typedef struct {
     int windowMode;              /* MYERS_WINDOW_* */
     int path;                    /* MYERS_PATH_* (default batched) */
     uint32_t maxQuerySize;       /* longest read accepted (0: 1024 bases) */
-    uint32_t laneWords;          /* 0: throughput shapes; k > 0: spread a read of more than k
-                                    32-bit words over several lanes of at most k words each (the
-                                    cheapest such shape), which cuts its time on the GPU
-                                    (latency) for some more work */
+    uint32_t laneWords;          /* 0: shapes by batch size, as myersVerifyAsync picks them on the
+                                    batched path (batches under 280K candidates run reads of up to
+                                    1,024 bases on lanes of at most 12 words); k > 0: spread a read
+                                    of more than k 32-bit words over several lanes of at most k
+                                    words each (the cheapest such shape), which cuts its time on
+                                    the GPU (latency) for some more work */
     int useGraphs;               /* non-zero: capture each batch's copies and kernels and replay them
                                     as a CUDA graph (updated in place batch to batch) */
 } myersServerConfig_t;
