@@ -47,13 +47,6 @@ static constexpr uint32_t kTbNotTraced = 0xFFFFFFFFu;
 static constexpr uint32_t kTbInconsistent = 0xFFFFFFFEu;
 static constexpr uint32_t kOpEq = 7, kOpX = 8, kOpI = 1, kOpD = 2;  // SAM codes
 
-// What the walk loads ahead (bits): 1 the next text word; 2 the next query
-// word's PEQ words; 4 the band entries where a diagonal path enters the next
-// query word, into L2.
-#ifndef MYERS_TB_PREFETCH
-#define MYERS_TB_PREFETCH 0
-#endif
-
 // Columns the walk fetches ahead of the one it is in.
 #ifndef MYERS_TB_AHEAD
 #define MYERS_TB_AHEAD 4
@@ -414,15 +407,6 @@ __device__ __forceinline__ TbCol tb_fetch(const uint4* __restrict__ slot, const 
   return c;
 }
 
-// Brings word x of column j1's band into L2 (nothing when it is not stored).
-__device__ __forceinline__ void tb_prefetch(const uint4* __restrict__ slot, const TbGeom& g, uint32_t j1, uint32_t x) {
-  if (j1 >= 1u && j1 >= g.a0 && j1 <= g.c1) {
-    const uint32_t xa = tb_xlo(g, j1);
-    if (x >= xa && x < xa + g.B)
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(slot + (size_t)(j1 - g.a0) * g.B + (x - xa))));
-  }
-}
-
 // The walk of list place k (a traced candidate of this chunk).
 __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
   const uint32_t id = a.ids[k];
@@ -443,10 +427,6 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
   uint32_t qw = 0xFFFFFFFFu, q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
   unsigned long long twi = ~0ull;
   uint32_t twv = 0;
-  // the walk goes up and left: the PEQ words of query word qw - 1 and text
-  // word twi - 1 come next, loaded when the current ones are
-  uint32_t n0 = 0, n1 = 0, n2 = 0, n3 = 0, n4 = 0, tnext = 0;
-  uint32_t pf_x = 0xFFFFFFFFu;  // the word whose next word's band entries were prefetched
   // every step lowers i or j1: at most m + c1 steps
   while (i > 0u) {
     uint32_t op;
@@ -460,15 +440,6 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
 #pragma unroll
         for (int d = 0; d <= D; ++d) cw[d] = tb_fetch(slot, g, j1 - (uint32_t)d, x);
       }
-#if MYERS_TB_PREFETCH & 4
-      // 8 rows before the word ends, the path (diagonal) will cross into word
-      // x - 1 near column j1 - 8: bring those entries into L2
-      if (sh == 8u && x > 0u && pf_x != x) {
-        pf_x = x;
-#pragma unroll
-        for (int d = 5; d <= 13; ++d) tb_prefetch(slot, g, j1 - (uint32_t)d, x - 1u);
-      }
-#endif
       if (cw[0].x != x) cw[0] = tb_fetch(slot, g, j1, x);
       if (cw[0].x != x) {  // the path left the stored band: the data is inconsistent
         bad = true;
@@ -476,46 +447,17 @@ __device__ void tb_walk_one(const TbArgs& a, uint32_t k) {
       }
       const uint32_t q = i - 1u;
       if ((q >> 5) != qw) {
-#if MYERS_TB_PREFETCH & 2
-        if ((q >> 5) + 1u == qw) {
-          q0 = n0;
-          q1 = n1;
-          q2 = n2;
-          q3 = n3;
-          q4 = n4;
-          qw = q >> 5;
-        } else {
-          qw = q >> 5;
-          q0 = qword(a.peq, g.pos_entry, nw, 0, (int)qw);
-          q1 = qword(a.peq, g.pos_entry, nw, 1, (int)qw);
-          q2 = qword(a.peq, g.pos_entry, nw, 2, (int)qw);
-          q3 = qword(a.peq, g.pos_entry, nw, 3, (int)qw);
-          q4 = qword(a.peq, g.pos_entry, nw, 4, (int)qw);
-        }
-        n0 = qword(a.peq, g.pos_entry, nw, 0, (int)qw - 1);
-        n1 = qword(a.peq, g.pos_entry, nw, 1, (int)qw - 1);
-        n2 = qword(a.peq, g.pos_entry, nw, 2, (int)qw - 1);
-        n3 = qword(a.peq, g.pos_entry, nw, 3, (int)qw - 1);
-        n4 = qword(a.peq, g.pos_entry, nw, 4, (int)qw - 1);
-#else
         qw = q >> 5;
         q0 = qword(a.peq, g.pos_entry, nw, 0, (int)qw);
         q1 = qword(a.peq, g.pos_entry, nw, 1, (int)qw);
         q2 = qword(a.peq, g.pos_entry, nw, 2, (int)qw);
         q3 = qword(a.peq, g.pos_entry, nw, 3, (int)qw);
         q4 = qword(a.peq, g.pos_entry, nw, 4, (int)qw);
-#endif
       }
       const unsigned long long b = g.start + j1 - 1u;
       if ((b >> 3) != twi) {
-#if MYERS_TB_PREFETCH & 1
-        twv = sanitize_codes((b >> 3) + 1ull == twi ? tnext : ref_load(a.ref, (long long)(b >> 3), a.ref_words));
-        twi = b >> 3;
-        tnext = ref_load(a.ref, (long long)twi - 1, a.ref_words);
-#else
         twi = b >> 3;
         twv = sanitize_codes(ref_load(a.ref, (long long)twi, a.ref_words));
-#endif
       }
       const uint32_t code = (twv >> (4u * (uint32_t)(b & 7u))) & 0xFu;
       const uint32_t pq = code == 0 ? q0 : code == 1 ? q1 : code == 2 ? q2 : code == 3 ? q3 : q4;
