@@ -559,7 +559,8 @@ def run_configs(mg, ms, args, ref3, peak, tmp, threads, padded3):
     """The benchmark's other configurations, each on the same GPU in this run:
     plain-100b (with its e2e), batched-mixed on both paths at full size and at
     110K candidates (with the batched path's e2e), batched-long on both paths,
-    and a short serving sweep. Steps per configuration are capped so the whole
+    the cut-off on plain-1000b and batched-mixed, the traceback of
+    plain-1000b, and a short serving sweep. Steps per configuration are capped so the whole
     line stays within a few minutes."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
@@ -628,6 +629,9 @@ def run_configs(mg, ms, args, ref3, peak, tmp, threads, padded3):
                            205, cutoff=0.08)
     out["plain-1000b-cutoff-0.08"] = {"workload": WORKLOAD_NAMES[2] + ", Ukkonen's cut-off at 0.08 m",
                                       "cutoff": 0.08, **cut}
+    # traceback of plain-1000b: the alignments of the candidates scoring at most 0.2 m
+    out["traceback-plain-1000b"] = {"workload": "traceback of " + WORKLOAD_NAMES[2],
+                                    **traceback_record(mg, ref3, rw, rs, w2, min(steps, 5), warmup, 16.0, 0.2)}
     del w2
 
     # batched-mixed under the cut-off at 0.08 m: the two passes as two
@@ -667,6 +671,7 @@ def targets_summary(value_plain_1000b, configs):
         "reference_parity_candidates": int(sum(p["candidates"] for p in samples)),
         "bit_exact_everywhere": all(p["bit_exact"] for p in samples) and all(same),
         "plain_1000b_cand_s": value_plain_1000b,
+        "traceback_plain_1000b_alignments_s": configs["traceback-plain-1000b"]["value"],
     }
 
 
@@ -887,21 +892,16 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
-def run_traceback(args):
-    """Traceback of the candidates whose score is within the bound: one step
-    = one myersTraceback call over the verified batch (selection, the
-    band-storing forward pass and the walk), inputs and results resident."""
+def traceback_record(mg, ref, ref_words, ref_size, w, steps, warmup, scratch_gb, bound):
+    """Traceback of the candidates whose score is within bound x the longest
+    read: one step = one myersTraceback call over the verified batch
+    (selection, the band-storing forward pass and the walk), inputs and
+    results resident. Returns the timing, roofline, parity and CPU-baseline
+    fields of a record."""
     import torch
-
-    import myersgpu as mg
-    import myerssynth as ms
-    torch.cuda.set_device(0)
-    k = args.workload
-    s, ref_words, ref_size, w = make_inputs(ms, k, args.scale, 0)
     n = len(w["cands"])
     m_of = w["qinfo"]["size"][w["cands"]["query"]].astype(np.int64)
-    max_score = int(args.tb_bound * int(m_of.max()))
-    ref = mg.Reference(ref_words, ref_size)
+    max_score = int(bound * int(m_of.max()))
     ctx = mg.Context(n)
 
     def dev(a):
@@ -917,34 +917,40 @@ def run_traceback(args):
     max_ops = 256  # runs per candidate: about 2 per edit of a traced alignment, plus one
     d_ops = torch.empty(n * max_ops, dtype=torch.int32, device="cuda")
     d_aln = torch.empty(n * 16, dtype=torch.uint8, device="cuda")
-    tb = mg.Traceback(n, int(args.tb_scratch_gb * (1 << 30)))
+    tb = mg.Traceback(n, int(scratch_gb * (1 << 30)))
+    try:
+        def step():
+            return tb.run(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(),
+                          d_res.data_ptr(), n, DIST, max_score, d_ops.data_ptr(), max_ops, d_aln.data_ptr(),
+                          stream=stream.cuda_stream)
 
-    def step():
-        return tb.run(ref, d_peq.data_ptr(), len(w["peq"]), d_qi.data_ptr(), len(w["qinfo"]), d_c.data_ptr(),
-                      d_res.data_ptr(), n, DIST, max_score, d_ops.data_ptr(), max_ops, d_aln.data_ptr(),
-                      stream=stream.cuda_stream)
-
-    for _ in range(args.warmup):
-        traced = step()
-    torch.cuda.synchronize()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    clocks = ClockSampler(0)
-    clocks.start()
-    times = []
-    for _ in range(args.steps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        traced = step()
-        b.record(stream)
-        clocks.poke()
+        for _ in range(warmup):
+            traced = step()
         torch.cuda.synchronize()
-        times.append(a.elapsed_time(b) / 1e3)
-    clk = clocks.stop()
-    del flush
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        clocks = ClockSampler(0)
+        clocks.start()
+        times = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            traced = step()
+            b.record(stream)
+            clocks.poke()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b) / 1e3)
+        clk = clocks.stop()
+        del flush
+        chunks = int(tb.chunks())
+    finally:
+        tb.close()
+        ctx.close()
     t = float(np.mean(times))
     aln = d_aln.cpu().numpy().view(mg.ALN)
     ops = d_ops.cpu().numpy().view(np.uint32).reshape(n, max_ops)
+    del d_peq, d_qi, d_c, d_res, d_ops, d_aln
+    torch.cuda.empty_cache()
     sel = (res["score"] != mg.NO_RESULT) & (res["score"] <= max_score)
     # work of the forward pass: ceil(m/32) words x (end column + 1) columns per traced candidate
     ws = float((np.ceil(m_of[sel] / 32.0) * (res["column"][sel].astype(np.float64) + 1)).sum())
@@ -968,16 +974,10 @@ def run_traceback(args):
     orc.traceback(w["peq"], w["qinfo"], w["cands"][sample], res[sample], ref_words, ref_size, DIST, max_score,
                   max_ops, nthreads=cores)
     cpu_s = time.perf_counter() - t0
-    chunks = int(tb.chunks())
-    ctx.close()
-    ref.close()
-    tb.close()
-    line = {
-        "metric": "alignments/s", "value": traced / t, "unit": "alignments/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
-        "config": {"workload": "traceback of " + WORKLOAD_NAMES[k], "traced": int(traced), "candidates": n,
-                   "max_score": max_score, "max_ops": max_ops, "scratch_gib": args.tb_scratch_gb, "l2": L2_NOTE},
+    return {
+        "value": traced / t, "unit": "alignments/s", "ms_per_step": t * 1e3, "steps": steps, "warmup": warmup,
+        "traced": int(traced), "candidates": n, "max_score": max_score, "max_ops": max_ops,
+        "scratch_gib": scratch_gb,
         "roofline": {"bound": "int32-alu", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s",
                      "frac": achieved / peak, "traffic": None,
                      "note": "whole call (selection, host read of the count, forward pass, walk) against the "
@@ -985,8 +985,34 @@ def run_traceback(args):
         "cpu_baseline": {"value": len(sample) / cpu_s, "unit": "alignments/s", "cores": cores, "kind": "port",
                          "sample": f"{len(sample)} traced candidates, the oracle's O(mn) DP traceback"},
         "parity_sample": {"candidates": int(len(pick)), "bit_exact": bool(ok)},
-        "ops_overflow": overflow,
-        "clocks": clk, "gpu_launches": 1 + 2 * chunks,
+        "ops_overflow": overflow, "clocks": clk, "gpu_launches": 1 + 2 * chunks,
+    }
+
+
+def run_traceback(args):
+    """The traceback line for one workload (--traceback)."""
+    import torch
+
+    import myersgpu as mg
+    import myerssynth as ms
+    torch.cuda.set_device(0)
+    k = args.workload
+    _, ref_words, ref_size, w = make_inputs(ms, k, args.scale, 0)
+    ref = mg.Reference(ref_words, ref_size)
+    try:
+        r = traceback_record(mg, ref, ref_words, ref_size, w, args.steps, args.warmup, args.tb_scratch_gb,
+                             args.tb_bound)
+    finally:
+        ref.close()
+    line = {
+        "metric": "alignments/s", "value": r["value"], "unit": "alignments/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+        "config": {"workload": "traceback of " + WORKLOAD_NAMES[k], "traced": r["traced"], "candidates": r["candidates"],
+                   "max_score": r["max_score"], "max_ops": r["max_ops"], "scratch_gib": r["scratch_gib"],
+                   "l2": L2_NOTE},
+        **{key: r[key] for key in ("roofline", "cpu_baseline", "parity_sample", "ops_overflow", "clocks",
+                                   "gpu_launches")},
     }
     print(json.dumps(line), flush=True)
 
