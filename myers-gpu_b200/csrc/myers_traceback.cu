@@ -109,11 +109,8 @@ struct TbGeom {
 
 // Words per lane for queries of up to `words` words: 8 up to 256 words
 // (8192 bases), then doubling, so that a query takes at most 32 lanes.
-#ifndef MYERS_TB_MIN_WL
-#define MYERS_TB_MIN_WL 8u
-#endif
 static inline uint32_t tb_words_per_lane(uint32_t words) {
-  uint32_t wl = MYERS_TB_MIN_WL;
+  uint32_t wl = 8;
   while (32u * wl < words) wl <<= 1;
   return wl;
 }
