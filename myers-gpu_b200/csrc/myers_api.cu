@@ -342,7 +342,8 @@ static Shape pick_shape(uint32_t w, bool batched, uint32_t lane_words = 0, bool 
 
 // Build the plan for the word counts flagged in `present` (size kMaxWords+1).
 // Uses fixed-size stack arrays only: no allocation on the send path.
-int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words, uint64_t n) {
+int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words, uint64_t n,
+                      uint64_t reads) {
   memset(&t, 0, sizeof(t));
   memset(t.cfg_of_words, kNoCfg, sizeof(t.cfg_of_words));
   Shape shapes[kMaxCfg];
@@ -351,9 +352,16 @@ int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32
   int nshapes = 0;
   for (uint32_t w = 0; w <= kMaxWords; ++w) cfg_of[w] = -1;
   const bool small = batched && lane_words == 0 && small_batch(n);
+  // Fewer than two candidates per read: a warp of 32 one-lane candidates then
+  // holds more distinct reads than the 16 PEQ slots of the single-lane shapes
+  // of more than 16 words, and runs its lanes in two rounds. Lanes of at most
+  // 16 words stage each lane's own words instead.
+  const bool distinct = lane_words == 0 && reads > 0 && n < 2 * reads;
   for (uint32_t w = 1; w <= kMaxWords; ++w) {
     if (!present[w]) continue;
-    const uint32_t lw = (small && w <= 32) ? kSmallBatchLaneWords : lane_words;
+    uint32_t lw = lane_words;
+    if (small && w <= 32) lw = kSmallBatchLaneWords;
+    else if (distinct && w > kDistinctLaneWords && w <= 32) lw = kDistinctLaneWords;
     const Shape s = pick_shape(w, batched, lw, large_batch(n));
     if (s.L == 0) return MYERS_E_QUERY_TOO_LONG;
     int found = -1;
@@ -490,7 +498,8 @@ int myers::cutoff_plans(PlanTable& plan, PlanTable& plan2, const uint8_t* presen
     if (r < m) w2[(m + 31) / 32] = 1;
   }
   const int st = build_plan(plan, w1, batched, 0, n);
-  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, batched, 0, n);
+  // the second pass holds the candidates that survived, mostly one per read
+  return st != MYERS_SUCCESS ? st : build_plan(plan2, w2, batched, 0, n, n);
 }
 
 extern "C" uint32_t myersContextLastLaunches(const myersContext_t* c) { return c ? c->last_launches : 0; }
@@ -639,14 +648,15 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
   return MYERS_SUCCESS;
 }
 
-static int plan_for_range(PlanTable& plan, uint32_t minSize, uint32_t maxSize, int path, uint64_t n) {
+static int plan_for_range(PlanTable& plan, uint32_t minSize, uint32_t maxSize, int path, uint64_t n,
+                          uint64_t reads) {
   uint8_t present[kMaxWords + 1];
   memset(present, 0, sizeof(present));
   if (maxSize == 0) maxSize = kMaxWords * 32;
   if (maxSize > kMaxWords * 32) maxSize = kMaxWords * 32;
   const uint32_t wlo = minSize ? (minSize + 31) / 32 : 1, whi = (maxSize + 31) / 32;
   for (uint32_t w = wlo; w <= whi; ++w) present[w] = 1;
-  return build_plan(plan, present, path == MYERS_PATH_BATCHED, 0, n);
+  return build_plan(plan, present, path == MYERS_PATH_BATCHED, 0, n, reads);
 }
 
 extern "C" int myersVerifyAsync(myersContext_t* ctx, const myersReference_t* ref, const qryEntry_t* d_peq,
@@ -711,7 +721,7 @@ static int verify_range(myersContext_t* ctx, const myersReference_t* ref, const 
     st = cutoff_plans(plan, plan2, present_m.data(), cutoff, mult, path == MYERS_PATH_BATCHED, numCandidates);
     if (st == MYERS_SUCCESS) st = ensure_cutoff_scratch(ctx);
   } else {
-    st = plan_for_range(plan, minQuerySize, maxQuerySize, path, numCandidates);
+    st = plan_for_range(plan, minQuerySize, maxQuerySize, path, numCandidates, numQueries);
   }
   if (st != MYERS_SUCCESS) return st;
   DevInputs in;
@@ -1061,7 +1071,7 @@ extern "C" int myersSend(void* mb, float distance, uint32_t numPEQEntries, uint3
       st = cutoff_plans(plan, b->plan2, pm.data(), b->cutoff, cutoff_prefix_mult(), b->path == MYERS_PATH_BATCHED,
                         numCandidates);
     } else {
-      st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED, 0, numCandidates);
+      st = build_plan(plan, present.data(), b->path == MYERS_PATH_BATCHED, 0, numCandidates, numQueries);
     }
   }
   if (st != MYERS_SUCCESS) return b->last_status = st;
@@ -1285,7 +1295,7 @@ extern "C" int myersVerifyNoAllocAsync(const uint32_t* d_refWords, uint64_t refW
   int st = noalloc_setup(&dev);
   if (st != MYERS_SUCCESS) return st;
   PlanTable plan;
-  st = plan_for_range(plan, minQuerySize, maxQuerySize, MYERS_PATH_BATCHED, numCandidates);
+  st = plan_for_range(plan, minQuerySize, maxQuerySize, MYERS_PATH_BATCHED, numCandidates, numQueries);
   if (st != MYERS_SUCCESS) return st;
   BucketState* d_state = reinterpret_cast<BucketState*>(dev.scratch);
   uint32_t* d_ids = reinterpret_cast<uint32_t*>(dev.scratch + kNoAllocIdsOffset);

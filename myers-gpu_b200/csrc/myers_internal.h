@@ -74,6 +74,9 @@ constexpr uint64_t kLargeBatchCandidates = 150000;
 // for reads of up to 1,024 bases: lanes of at most kSmallBatchLaneWords words.
 constexpr uint64_t kSmallBatchCandidates = 280000;
 constexpr uint32_t kSmallBatchLaneWords = 12;
+// With fewer than two candidates per read, reads of 513..1,024 bases take
+// lanes of at most this many words.
+constexpr uint32_t kDistinctLaneWords = 16;
 constexpr uint8_t kNoCfg = 0xFF;
 
 // Per-send plan, passed by value as a __grid_constant__ kernel parameter:
@@ -207,7 +210,9 @@ cudaError_t launch_lop3_probe(uint32_t* d_out, int blocks, int threads, int iter
 // Shape plan for the word counts flagged in present[0..kMaxWords].
 // n: the batch's candidates, which picks the batched path's table for large
 // batches at kLargeBatchCandidates or more.
-int build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words = 0, uint64_t n = 0);
+// reads: how many reads the n candidates come from (0: unknown).
+int build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32_t lane_words = 0, uint64_t n = 0,
+               uint64_t reads = 0);
 // Upper bound of the persistent kernel's tiles for n candidates under `plan`.
 uint32_t batched_tile_bound(const PlanTable& plan, uint32_t n);
 // Record a CUDA failure (message for myersGetErrorString) and return MYERS_E_CUDA.

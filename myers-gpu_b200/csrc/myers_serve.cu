@@ -151,7 +151,7 @@ static int dispatch_slot(myersServer* srv, Slot& s) {
   }
   s.ncands = nc;
   PlanTable plan;
-  int st = build_plan(plan, present, srv->cfg.path == MYERS_PATH_BATCHED, srv->cfg.laneWords, nc);
+  int st = build_plan(plan, present, srv->cfg.path == MYERS_PATH_BATCHED, srv->cfg.laneWords, nc, nq);
   if (st != MYERS_SUCCESS) return st;
   // With graphs, the batch's copies and kernels are captured and replayed as
   // one graph, updated in place from the slot's previous batch.
