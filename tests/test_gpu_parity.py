@@ -323,6 +323,22 @@ def test_concurrent_contexts_on_two_streams(gpu, orc, workloads):
         ref.close()
 
 
+@pytest.mark.parametrize("path", ["plain", "batched"])
+def test_one_candidate_per_read(gpu, orc, workloads, path):
+    """With fewer than two candidates per read, reads of 513..1,024 bases run
+    on lanes of at most 16 words (a warp's 32 candidates then come from 32
+    reads, more than the 16 PEQ slots of one-lane shapes of more than 16
+    words): every 11th candidate of 1,000-base and mixed reads."""
+    ref, ref_size, ws = workloads
+    p = gpu.PATH_PLAIN if path == "plain" else gpu.PATH_BATCHED
+    for k in (2, 3):
+        w = ws[k]
+        sel = np.ascontiguousarray(w["cands"][::11])
+        assert len(sel) < 2 * len(w["qinfo"])
+        res, _, _ = _run(gpu, ref, ref_size, w["peq"], w["qinfo"], sel, gpu.WINDOW_ALIGNED, p)
+        assert np.array_equal(res, orc.verify(w["peq"], w["qinfo"], sel, ref, ref_size, DIST)), k
+
+
 @pytest.mark.parametrize("env", [{"MYERS_LARGE_BATCH": "1", "MYERS_SMALL_BATCH": "0"},
                                  {"MYERS_SMALL_BATCH": "0"}], ids=["large", "tuned"])
 def test_batch_size_shapes(env):
