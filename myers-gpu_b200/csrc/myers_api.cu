@@ -268,6 +268,17 @@ static bool large_batch(uint64_t n) {
   return n >= threshold;
 }
 
+// How many of a context's streams the plain path spreads its launches over
+// (MYERS_PLAIN_STREAMS, 1..kPlainStreams; 1 keeps them on the caller's stream).
+static int plain_streams() {
+  static const int k = [] {
+    const char* env = getenv("MYERS_PLAIN_STREAMS");
+    const int v = env ? atoi(env) : kPlainStreams;
+    return v < 1 ? 1 : (v > kPlainStreams ? kPlainStreams : v);
+  }();
+  return k;
+}
+
 // Whether a batch of n candidates on the batched path takes latency shapes
 // (lanes of at most kSmallBatchLaneWords words) for reads of up to 1,024
 // bases. A small batch runs about one wave of tiles and ends with its longest
@@ -409,6 +420,17 @@ int myers::build_plan(PlanTable& t, const uint8_t* present, bool batched, uint32
 // context: device scratch for bucketing
 
 
+static void destroy_plain_streams(myersContext* c) {
+  for (int i = 0; i < kPlainStreams; ++i) {
+    if (c->aux[i]) cudaStreamDestroy(c->aux[i]);
+    if (c->join[i]) cudaEventDestroy(c->join[i]);
+    c->aux[i] = nullptr;
+    c->join[i] = nullptr;
+  }
+  if (c->fork) cudaEventDestroy(c->fork);
+  c->fork = nullptr;
+}
+
 extern "C" int myersContextCreate(myersContext_t** out, uint64_t maxCandidates) {
   if (out == nullptr || maxCandidates > 0xFFFFFFFFull) return MYERS_E_INVALID_ARGUMENT;
   myersContext* c = new myersContext();
@@ -430,6 +452,16 @@ extern "C" int myersContextCreate(myersContext_t** out, uint64_t maxCandidates) 
     delete c;
     return e == cudaErrorMemoryAllocation ? MYERS_E_INSUFFICIENT_MEM_GPU : cuda_fail(e, "context");
   }
+  // The plain path's streams. Without them its launches stay on the caller's
+  // stream, one after another.
+  bool streams = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < kPlainStreams && streams; ++i)
+    streams = cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!streams) {
+    destroy_plain_streams(c);
+    cudaGetLastError();
+  }
   *out = c;
   return MYERS_SUCCESS;
 }
@@ -446,6 +478,7 @@ extern "C" int myersContextDestroy(myersContext_t* c) {
   cudaFree(c->d_esc_ids);
   cudaFree(c->d_esc_cfg);
   cudaFree(c->d_esc_state);
+  destroy_plain_streams(c);
   cudaSetDevice(cur);
   delete c;
   return MYERS_SUCCESS;
@@ -538,6 +571,31 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     const Shape sh = plan.shape[c];
     return launch_plain(sh.variant, sh.L, in, ids, st, (int)c, 0, count, next, s, ctx->num_sms);
   };
+  // Plain launches of shapes c0..c1-1 of `pl` over the lists in `st`. With
+  // more than one shape they are spread over the context's streams, forked
+  // from s and joined back to it: each launch ends in a partial wave, which
+  // the other shapes' launches fill.
+  auto plain_range = [&](const PlanTable& pl, const DevInputs& din, uint32_t c0, uint32_t c1, const uint32_t* ids,
+                         BucketState* st) -> cudaError_t {
+    const uint32_t k = c1 - c0 < (uint32_t)plain_streams() ? c1 - c0 : (uint32_t)plain_streams();
+    cudaError_t e = cudaSuccess;
+    if (k <= 1 || ctx->aux[0] == nullptr) {
+      for (uint32_t c = c0; c < c1 && e == cudaSuccess; ++c)
+        e = launch_plain(pl.shape[c].variant, pl.shape[c].L, din, ids, st, (int)c, 0, 0, &st->next[c], s,
+                         ctx->num_sms);
+      return e;
+    }
+    e = cudaEventRecord(ctx->fork, s);
+    for (uint32_t i = 0; i < k && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(ctx->aux[i], ctx->fork, 0);
+    for (uint32_t c = c0; c < c1 && e == cudaSuccess; ++c)
+      e = launch_plain(pl.shape[c].variant, pl.shape[c].L, din, ids, st, (int)c, 0, 0, &st->next[c],
+                       ctx->aux[(c - c0) % k], ctx->num_sms);
+    for (uint32_t i = 0; i < k && e == cudaSuccess; ++i) {
+      e = cudaEventRecord(ctx->join[i], ctx->aux[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->join[i], 0);
+    }
+    return e;
+  };
   if (in.cut && path == MYERS_PATH_BATCHED && plan2 != nullptr) {
     // The cut-off's two passes as two persistent launches: the first over
     // the prefixes' tiles (plan), then the tile layout of the lists it filled,
@@ -607,19 +665,13 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
       launches += (uint32_t)launch_bucketing_cutoff(in, plan, *plan2, ctx->d_state, ctx->d_cfg, ctx->d_ids, s,
                                                     ctx->num_sms, &e);
       if (e != cudaSuccess) return cuda_fail(e, "bucketing");
-      for (uint32_t c = 0; c < plan.num_cfg; ++c) {
-        CU(plain(c, ctx->d_ids, ctx->d_state, 0, &ctx->d_state->next[c]));
-        ++launches;
-      }
+      CU(plain_range(plan, in, 0, plan.num_cfg, ctx->d_ids, ctx->d_state));
+      launches += plan.num_cfg;
     }
     DevInputs in2 = in;
     in2.prefix = 0;
-    for (uint32_t c = 0; c < plan2->num_cfg; ++c) {
-      const Shape sh = plan2->shape[c];
-      CU(launch_plain(sh.variant, sh.L, in2, ctx->d_esc_ids, ctx->d_esc_state, (int)c, 0, 0,
-                      &ctx->d_esc_state->next[c], s, ctx->num_sms));
-      ++launches;
-    }
+    CU(plain_range(*plan2, in2, 0, plan2->num_cfg, ctx->d_esc_ids, ctx->d_esc_state));
+    launches += plan2->num_cfg;
     ctx->last_launches = launches;
     return MYERS_SUCCESS;
   }
@@ -640,10 +692,8 @@ int myers::verify_enqueue(myersContext* ctx, const myersReference* ref, const De
     ++launches;
     first_plain = plan.num_batched;
   }
-  for (uint32_t c = first_plain; c < plan.num_cfg; ++c) {
-    CU(plain(c, ctx->d_ids, ctx->d_state, 0, &ctx->d_state->next[c]));
-    ++launches;
-  }
+  CU(plain_range(plan, in, first_plain, plan.num_cfg, ctx->d_ids, ctx->d_state));
+  launches += plan.num_cfg - first_plain;
   ctx->last_launches = launches;
   return MYERS_SUCCESS;
 }

@@ -77,6 +77,8 @@ constexpr uint32_t kSmallBatchLaneWords = 12;
 // With fewer than two candidates per read, reads of 513..1,024 bases take
 // lanes of at most this many words.
 constexpr uint32_t kDistinctLaneWords = 16;
+// Streams a context's plain launches of different shapes run on at once.
+constexpr int kPlainStreams = 4;
 constexpr uint8_t kNoCfg = 0xFF;
 
 // Per-send plan, passed by value as a __grid_constant__ kernel parameter:
@@ -241,6 +243,11 @@ struct myersContext {
   uint32_t* d_esc_ids;
   uint8_t* d_esc_cfg;
   myers::BucketState* d_esc_state;
+  // streams the plain path spreads its per-shape launches over (forked from
+  // and joined back to the caller's stream); null when they could not be made
+  cudaStream_t aux[myers::kPlainStreams];
+  cudaEvent_t fork;
+  cudaEvent_t join[myers::kPlainStreams];
 };
 
 namespace myers {
