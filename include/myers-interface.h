@@ -200,7 +200,10 @@ int myersReferenceDestroy(myersReference_t *ref);
 uint64_t myersReferenceSize(const myersReference_t *ref);
 
 /* Opaque per-stream work context: device scratch for length bucketing and
- * the work queue, sized for up to maxCandidates candidates. */
+ * the work queue, sized for up to maxCandidates candidates, and four streams
+ * the plain path runs its per-shape launches on (forked from the caller's
+ * stream and joined back to it; MYERS_PLAIN_STREAMS=1 keeps them on the
+ * caller's stream). */
 typedef struct myersContext myersContext_t;
 int myersContextCreate(myersContext_t **ctx, uint64_t maxCandidates);
 int myersContextDestroy(myersContext_t *ctx);
